@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark of the GLM-MHD time step on B200.
+
+Workload (one "step" = one full time step of the 512^3 periodic box, FP32): CFL reduction fused
+into the previous step's write-out, host dt/ch from it (as compute_dt does), OU mode forcing update
+on the reference cadence, and the fused unsplit PLM(MC) + MUSCL-Hancock + HLLD + Dedner GLM step
+with the forcing kick.  Initial state: seeded synthetic turbulence (rms Mach 1, gamma 5/3, rho 1,
+p 0.6, B0 = (0.775, 0, 0)) standing in for the pre-evolved checkpoint of the 512^3 configuration.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs under torchrun as independent replicas (the step has no cross-box exchange).
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 512
+AMP = 2.0            # forcing amplitude (stationary rms acceleration)
+COURANT = 0.3
+CP_COEF = 0.18
+GAMMA = 5.0 / 3.0
+BYTES_PER_ZONE = {"f32": 72, "f64": 144}   # read 9 + write 9 conserved reals per zone update
+PUBLISHED_A6000 = 0.902e9   # full step with fused OU forcing @512^3 FP32, RTX A6000 (REPORT.md:14)
+METRIC = "zone-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--recon", default="mc")
+    ap.add_argument("--riemann", default="hlld")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args, extra=None):
+    c = {"workload": f"glm_mhd_{args.n}^3_{args.dtype}_plm_{args.riemann}_glm_forcing", "n": args.n,
+         "scheme": "unsplit", "recon": args.recon, "riemann": args.riemann, "forcing": "ou_61_modes",
+         "gamma": GAMMA, "courant": COURANT, "ic": "seeded synthetic turbulence, Mach 1, seed 1",
+         "l2": "inputs larger than L2 (state %.2f GB per register)" % (args.n ** 3 * 9 * (4 if args.dtype == "f32" else 8) / 1e9)}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# --------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = os.path.join("/tmp", f"gmt_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def ncu_traffic(args):
+    """DRAM bytes per zone of the step kernel from the committed ncu summary (profiles/)."""
+    try:
+        t = json.load(open(os.path.join(ROOT, "profiles", "step_kernel_traffic.json")))
+        key = f"unsplit_{args.dtype}_{args.recon}_{args.riemann}"
+        return t[key]["dram_bytes_per_zone"], t[key].get("note", "")
+    except Exception:
+        return None, ""
+
+
+# --------------------------------------------------------------------------------------------
+def cpu_baseline_sample(dtype, recon, riemann, target_s=12.0):
+    """Oracle (C++ restatement, all host threads) on a bounded sample of the same scheme."""
+    import numpy as np
+    from oracle import oracle as O
+    nthr = O.set_threads(os.cpu_count() or 1)
+    np_dtype = np.float32 if dtype == "f32" else np.float64
+
+    def run(n, steps):
+        cfg = O.Config(n=(n, n, n), gamma=GAMMA, recon=recon, riemann=riemann, iflo=True)
+        u = O.ic_uniform(cfg, 1.0, 0.6, (0.775, 0.0, 0.0)).astype(np_dtype)
+        rng = np.random.default_rng(1)
+        u[1:4] += (0.5 * rng.standard_normal(u[1:4].shape)).astype(np_dtype)
+        f = O.OUForcing(amp=AMP, T=0.5, seed=1)
+        f.advance()
+        dt = 1e-4
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            u = O.step_unsplit(cfg, u, dt, 2.0, 0.99, 0.5, f.modes)
+        return time.perf_counter() - t0
+
+    t32 = run(32, 1)
+    per_zone = t32 / 32 ** 3
+    n = 32
+    for cand in (48, 64, 96, 128, 160, 192, 256):
+        if per_zone * cand ** 3 <= target_s / 2:
+            n = cand
+    steps = max(1, min(4, int(target_s / (per_zone * n ** 3))))
+    el = run(n, steps)
+    return {"value": n ** 3 * steps / el, "unit": METRIC, "cores": nthr, "kind": "port",
+            "sample": f"{steps} step(s) of the same scheme (PLM-{recon}+{riemann}+GLM+forcing, {dtype}) at {n}^3 "
+                      f"with the C++ oracle on {nthr} host threads"}
+
+
+# --------------------------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np
+    from oracle import oracle as O
+    nthr = O.set_threads(os.cpu_count() or 1)
+    np_dtype = np.float32 if args.dtype == "f32" else np.float64
+    # size one step of the sample to ~2 s so that K + W steps end within a few minutes
+    cfg32 = O.Config(n=(32, 32, 32), gamma=GAMMA, recon=args.recon, riemann=args.riemann)
+    u = O.ic_uniform(cfg32).astype(np_dtype)
+    t0 = time.perf_counter()
+    O.step_unsplit(cfg32, u, 1e-4, 2.0, 0.99)
+    per_zone = (time.perf_counter() - t0) / 32 ** 3
+    n = 32
+    for cand in (48, 64, 80, 96, 112, 128, 160, 192):
+        if per_zone * cand ** 3 <= 2.0:
+            n = cand
+    cfg = O.Config(n=(n, n, n), gamma=GAMMA, recon=args.recon, riemann=args.riemann, iflo=True)
+    u = O.ic_uniform(cfg, 1.0, 0.6, (0.775, 0.0, 0.0)).astype(np_dtype)
+    rng = np.random.default_rng(1)
+    u[1:4] += (0.5 * rng.standard_normal(u[1:4].shape)).astype(np_dtype)
+    f = O.OUForcing(amp=AMP, T=0.5, seed=1)
+    f.advance()
+    t = 0.0
+
+    def step(u, t):
+        while t >= f.next_time:
+            f.advance()
+        cmax, smax = O.cfl(cfg, u)
+        dt = min(COURANT * cfg.dx / cmax, f.next_time - t)
+        fac = math.exp(-(smax / CP_COEF) * dt)
+        return O.step_unsplit(cfg, u, dt, smax, fac, min(t / 0.5, 1.0), f.modes), t + dt
+
+    for _ in range(args.warmup):
+        u, t = step(u, t)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        u, t = step(u, t)
+    el = time.perf_counter() - t0
+    value = n ** 3 * args.steps / el
+    out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+           "impl": "reference",
+           "config": workload_config(args, {"sample_n": n}),
+           "cpu_baseline": {"value": value, "unit": METRIC, "cores": nthr, "kind": "port",
+                            "sample": f"each step = one step of the same scheme at {n}^3 (CFL + forcing + "
+                                      f"PLM-{args.recon}+{args.riemann}+GLM) with the C++ oracle"},
+           "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    # the CPU baseline runs before any GPU work of this process (OpenMP threads, no fork)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(args.dtype, args.recon, args.riemann)
+
+    from glmmhdturb_b200 import Solver
+    n = args.n
+    s = Solver(n, dtype=args.dtype, recon=args.recon, riemann=args.riemann, gamma=GAMMA, courant=COURANT,
+               turb_amp=AMP, turb_T=0.5, turb_ndt=100, turb_seed=1)
+    stream = torch.cuda.current_stream()
+    u = s.alloc()
+    w = s.alloc()
+    s.ic_turbulent(u, 1.0, 0.6, (0.775, 0.0, 0.0), mach=1.0, db=0.1, seed=1)
+    zones = s.n
+    state_bytes = u.numel() * u.element_size()
+    st = {"t": 0.0, "launches": 0}
+
+    def begin():
+        s.forcing_reset()
+        s.forcing_advance()
+        st["t"] = 0.0
+        st["cm"], st["sm"] = s.cfl(u)
+
+    kernel_events = []
+
+    def one_step(record):
+        nonlocal u, w
+        while st["t"] >= s.next_time:
+            s.forcing_advance()
+            st["launches"] += 2          # OU update + mode-table refresh
+        dt = min(COURANT * s.dx / st["cm"], s.next_time - st["t"])
+        ch = st["sm"]
+        fac = math.exp(-(ch / CP_COEF) * dt)
+        if record:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        s.step(u, w, dt, t=st["t"], ch=ch, glm_fac=fac, do_turb=True, want_cfl=True)
+        if record:
+            e1.record(stream)
+            kernel_events.append((e0, e1))
+        st["launches"] += 1
+        st["cm"], st["sm"] = s.cfl_result()   # dt of the next step needs this scalar on the host
+        u, w = w, u
+        st["t"] += dt
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---------------- device-resident run
+    begin()
+    for _ in range(args.warmup):
+        one_step(False)
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    st["launches"] = 0
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        one_step(True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = st["launches"]
+    kms = [a.elapsed_time(b) for a, b in kernel_events]
+    kmean = sum(kms) / len(kms)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    diag = s.diagnostics(u)
+
+    # ---------------- end to end through the public API from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.empty(u.shape, dtype=u.dtype, pin_memory=True)
+        s.ic_turbulent(w, 1.0, 0.6, (0.775, 0.0, 0.0), mach=1.0, db=0.1, seed=1)
+        host_in.copy_(w)
+        host_out = torch.empty_like(host_in, pin_memory=True)
+        torch.cuda.synchronize()
+        barrier()
+        x0 = torch.cuda.Event(enable_timing=True)
+        x1 = torch.cuda.Event(enable_timing=True)
+        x0.record(stream)
+        u.copy_(host_in, non_blocking=True)
+        begin()
+        for _ in range(args.steps):
+            one_step(False)
+        host_out.copy_(u, non_blocking=True)
+        x1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ems = x0.elapsed_time(x1)
+        if world > 1:
+            tt = torch.tensor([ems], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        e2e = {"value": world * zones * args.steps / (ems * 1e-3), "unit": METRIC,
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": state_bytes / args.steps + 16,
+               "note": "initial state uploaded from pinned host memory, K steps with the per-step CFL "
+                       "scalars read back for dt (16 B), final state downloaded; all inside the timed region"}
+
+    if rank == 0:
+        peaks = measured_peaks()
+        peak = peaks.get("hbm_gbs")
+        peak_src = "measured" if peak else "fallback"
+        peak = peak or 6650.0
+        alg = BYTES_PER_ZONE[args.dtype] * zones
+        achieved = alg / (kmean * 1e-3) / 1e9
+        tb, note = ncu_traffic(args)
+        value = world * zones * args.steps / (ms * 1e-3)
+        info = s.kernel_info()
+        out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": value / PUBLISHED_A6000, "dtype": args.dtype,
+               "data": "synthetic",
+               "config": workload_config(args, {"parallelism": f"replicas{world}" if world > 1 else "single",
+                                                "tile": list(info["tile"]), "regs": info["regs"],
+                                                "smem_bytes": info["smem"]}),
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "peak_source": peak_src,
+                            "traffic": (tb * zones if tb else None),
+                            "kernel_ms": kmean,
+                            "algorithmic_bytes_per_launch": alg,
+                            "traffic_note": note},
+               "gpu_launches": launches,
+               "clocks": clk,
+               "e2e": e2e,
+               "diagnostics": {k: diag[k] for k in ("vrms", "divbmax", "rhomin", "finite")}}
+        if cpu is not None:
+            out["cpu_baseline"] = cpu
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,707 @@
+// gmt_api.cu -- C ABI of libglmmhd_b200.so (declared in include/glmmhd_b200.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/glmmhd_b200.h"
+#include "gmt_internal.h"
+#include "gmt_unsplit.cuh"
+
+using namespace gmt;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char* where) {
+    g_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return GMT_ERR_CUDA;
+}
+#define GMT_CUDA(call)                                           \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);      \
+    } while (0)
+
+const double kTwoPi = 6.283185307179586476925286766559;
+
+std::vector<double> trig_table(int n) {
+    std::vector<double> t(8 * (size_t)n);
+    for (int m = 0; m < 4; ++m)
+        for (int i = 0; i < n; ++i) {
+            double th = kTwoPi * (double)m * ((double)i + 0.5) / (double)n;
+            t[(size_t)(2 * m) * n + i] = std::cos(th);
+            t[(size_t)(2 * m + 1) * n + i] = std::sin(th);
+        }
+    return t;
+}
+
+// sigma0 such that the stationary rms |a| equals amp, sqrt(P(k)) = 1/|k|
+double forcing_sigma0(double amp, double alpha, double beta) {
+    double s = 0.0;
+    for (int kx = 0; kx <= 3; ++kx)
+        for (int ky = -3; ky <= 3; ++ky)
+            for (int kz = -3; kz <= 3; ++kz) {
+                int k2 = kx * kx + ky * ky + kz * kz;
+                bool half = kx > 0 || (kx == 0 && ky > 0) || (kx == 0 && ky == 0 && kz > 0);
+                if (k2 >= 1 && k2 <= 9 && half) s += 1.0 / k2;
+            }
+    return amp * std::sqrt((1.0 - alpha * alpha) / (8.0 * beta * beta * s));
+}
+
+bool divides(int n, int t) { return t > 0 && n % t == 0; }
+
+}  // namespace
+
+struct gmt_ctx {
+    gmt_params p;
+    int device = 0;
+    int esize = 4;            // bytes per real
+    size_t n = 0;             // cells
+    int ox = 0, oy = 0, lz = 0;
+    unsigned long long* cfl = nullptr;   // [2]
+    double* diag_part = nullptr;
+    double* diag_out = nullptr;
+    int diag_blocks = 592;
+    double* modes = nullptr;  // [61][3][2]
+    void* btab = nullptr;     // [nz][ny][24] reals
+    void* trig[3] = {nullptr, nullptr, nullptr};
+    void* ct_scratch = nullptr;
+    unsigned long long* divb = nullptr;
+    uint32_t counter = 0;
+    double sigma0 = 0, alpha = 0, beta = 0;
+};
+
+namespace {
+
+template <class R> Consts<R> consts_of(const gmt_params& p) {
+    Consts<R> K;
+    K.gamma = (R)p.gamma;
+    K.smallr = (R)p.smallr;
+    K.smallc = (R)p.smallc;
+    K.pfl = K.smallr * (K.smallc * K.smallc) / K.gamma;
+    K.smallp = (R)p.smallp;
+    K.llf_dmin = (R)p.llf_dmin;
+    K.llf_pmin = (R)p.llf_pmin;
+    K.turb_min_rho = (R)p.turb_min_rho;
+    return K;
+}
+
+int choose_tile(gmt_ctx* c) {
+    const gmt_params& p = c->p;
+    static const int cand[][2] = {{32, 8}, {32, 4}, {16, 8}, {16, 4}, {8, 8}, {8, 4}, {4, 4}, {8, 2},
+                                  {4, 2}, {2, 2}, {8, 1}, {4, 1}, {2, 1}, {1, 1}};
+    int ox = p.tile_x, oy = p.tile_y;
+    if (ox <= 0 || oy <= 0) {
+        ox = oy = 0;
+        for (auto& t : cand)
+            if (divides(p.nx, t[0]) && divides(p.ny, t[1])) { ox = t[0]; oy = t[1]; break; }
+    }
+    if (!divides(p.nx, ox) || !divides(p.ny, oy))
+        return fail(GMT_ERR_ARG, "tile " + std::to_string(ox) + "x" + std::to_string(oy) + " does not divide the grid");
+    if (ox * oy > 256) return fail(GMT_ERR_ARG, "tile_x*tile_y must be <= 256");
+    if (unsplit_smem(c->esize, ox, oy) > 227 * 1024) return fail(GMT_ERR_ARG, "tile needs more than 227 KB shared memory");
+    int lz = p.tile_z;
+    if (lz <= 0) {
+        long cols = (long)(p.nx / ox) * (p.ny / oy);
+        lz = p.nz;
+        while (lz > 8 && cols * ((p.nz + lz - 1) / lz) < 148L * 8) lz = (lz + 1) / 2;
+    }
+    c->ox = ox; c->oy = oy; c->lz = std::min(lz, p.nz);
+    return GMT_OK;
+}
+
+template <class R> CPlanes<R> cplanes(const void* base, size_t n) {
+    CPlanes<R> P;
+    for (int v = 0; v < 9; ++v) P.p[v] = static_cast<const R*>(base) + (size_t)v * n;
+    return P;
+}
+template <class R> Planes<R> planes(void* base, size_t n) {
+    Planes<R> P;
+    for (int v = 0; v < 9; ++v) P.p[v] = static_cast<R*>(base) + (size_t)v * n;
+    return P;
+}
+
+template <class R>
+int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_step_args* a, cudaStream_t s) {
+    const gmt_params& p = c->p;
+    const double dx = p.boxlen / p.nx;
+    if (!(a->dt > 0.0) || !std::isfinite(a->dt)) return fail(GMT_ERR_ARG, "dt must be positive and finite");
+    if (p.scheme == GMT_SCHEME_UNSPLIT) {
+        if (!(a->ch > 0.0)) return fail(GMT_ERR_ARG, "ch must be positive");
+        UnsplitArgs<R> A;
+        A.u = u; A.o = o;
+        A.nx = p.nx; A.ny = p.ny; A.nz = p.nz;
+        A.ox = c->ox; A.oy = c->oy; A.lz = c->lz;
+        A.dt = (R)a->dt; A.dtdx = A.dt / (R)dx;
+        A.ch = (R)a->ch; A.glm_fac = (R)a->glm_fac;
+        A.ramp = (R)(p.turb_T > 0 ? std::min(a->t / p.turb_T, 1.0) : 1.0);
+        A.K = consts_of<R>(p);
+        A.iflo = p.iflo; A.use_llf = p.riemann == GMT_RIEMANN_LLF; A.do_turb = a->do_turb;
+        A.btab = a->do_turb ? static_cast<const R*>(c->btab) : nullptr;
+        A.trigx = static_cast<const R*>(c->trig[0]);
+        A.cfl_out = nullptr;
+        if (a->want_cfl) {
+            GMT_CUDA(cudaMemsetAsync(c->cfl, 0, 2 * sizeof(unsigned long long), s));
+            A.cfl_out = c->cfl;
+        }
+        int riem = p.riemann == GMT_RIEMANN_LLF ? GMT_RIEMANN_HLLD : p.riemann;
+        cudaError_t e = launch_unsplit(A, p.recon, riem, s);
+        if (e != cudaSuccess) return cuda_fail(e, "unsplit step");
+        return GMT_OK;
+    }
+    if (p.scheme == GMT_SCHEME_MARCH1D) {
+        MarchArgs<R> A;
+        A.u = u; A.o = o;
+        A.nx = p.nx; A.ny = p.ny; A.nz = p.nz;
+        A.ox = c->ox; A.oy = c->oy; A.lz = c->lz;
+        A.dtdx = (R)(a->dt / dx);
+        A.ch = (R)a->ch; A.glm_fac = (R)a->glm_fac;
+        A.K = consts_of<R>(p);
+        A.ppm = p.recon == GMT_RECON_PPM;
+        cudaError_t e = launch_march1d(A, s);
+        if (e != cudaSuccess) return cuda_fail(e, "march1d step");
+        if (a->want_cfl) {
+            e = launch_cfl<R>(CPlanes<R>{{o.p[0], o.p[1], o.p[2], o.p[3], o.p[4], o.p[5], o.p[6], o.p[7], o.p[8]}},
+                              c->n, A.K, c->cfl, s);
+            if (e != cudaSuccess) return cuda_fail(e, "cfl");
+        }
+        return GMT_OK;
+    }
+    return fail(GMT_ERR_ARG, "gmt_step: this context is a CT context; use gmt_ct_step");
+}
+
+template <class R> int refresh_btab(gmt_ctx* c, cudaStream_t s) {
+    cudaError_t e = launch_btab<R>(c->modes, static_cast<const R*>(c->trig[1]), static_cast<const R*>(c->trig[2]),
+                                   c->p.ny, c->p.nz, static_cast<R*>(c->btab), s);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "forcing table");
+}
+int refresh_btab_any(gmt_ctx* c, cudaStream_t s) {
+    return c->esize == 8 ? refresh_btab<double>(c, s) : refresh_btab<float>(c, s);
+}
+
+template <class R> CPlanes8<R> cplanes8(const void* base, size_t n) {
+    CPlanes8<R> P;
+    for (int v = 0; v < 8; ++v) P.p[v] = static_cast<const R*>(base) + (size_t)v * n;
+    return P;
+}
+template <class R> Planes8<R> planes8(void* base, size_t n) {
+    Planes8<R> P;
+    for (int v = 0; v < 8; ++v) P.p[v] = static_cast<R*>(base) + (size_t)v * n;
+    return P;
+}
+
+template <class R>
+int ct_step_impl(gmt_ctx* c, const CPlanes8<R>& q, const Planes8<R>& o, const gmt_step_args* a, cudaStream_t s) {
+    const gmt_params& p = c->p;
+    if (!(a->dt > 0.0) || !std::isfinite(a->dt)) return fail(GMT_ERR_ARG, "dt must be positive and finite");
+    CTArgs<R> A;
+    A.q = q; A.o = o;
+    A.nx = p.nx; A.ny = p.ny; A.nz = p.nz;
+    A.ox = c->ox; A.oy = c->oy; A.lz = c->lz;
+    A.dt = (R)a->dt;
+    A.dtdx = A.dt / (R)(p.boxlen / p.nx);
+    A.ramp = (R)(p.turb_T > 0 ? std::min(a->t / p.turb_T, 1.0) : 1.0);
+    A.K = consts_of<R>(p);
+    A.recon = p.recon; A.riem = p.riemann; A.emf = p.emf; A.halfslope = p.ct_halfslope;
+    A.do_turb = a->do_turb;
+    A.btab = a->do_turb ? static_cast<const R*>(c->btab) : nullptr;
+    A.trigx = static_cast<const R*>(c->trig[0]);
+    A.scratch = static_cast<R*>(c->ct_scratch);
+    cudaError_t e = launch_ct(A, s);
+    if (e != cudaSuccess) return cuda_fail(e, "ct step");
+    if (a->want_cfl) {
+        CPlanes8<R> oc;
+        for (int v = 0; v < 8; ++v) oc.p[v] = o.p[v];
+        e = launch_ct_cfl<R>(oc, p.nx, p.ny, p.nz, A.K, c->cfl, s);
+        if (e != cudaSuccess) return cuda_fail(e, "ct cfl");
+    }
+    return GMT_OK;
+}
+
+std::once_flag g_mode_once;
+cudaError_t g_mode_err = cudaSuccess;
+
+}  // namespace
+
+extern "C" {
+
+const char* gmt_version(void) { return "glmmhd_b200 1.0 (sm_100a)"; }
+const char* gmt_last_error(void) { return g_err.c_str(); }
+
+int gmt_params_init(gmt_params* p, int n) {
+    if (!p || n <= 0) return fail(GMT_ERR_ARG, "gmt_params_init: null params or n <= 0");
+    std::memset(p, 0, sizeof(*p));
+    p->abi_version = GMT_ABI_VERSION;
+    p->nx = p->ny = p->nz = n;
+    p->dtype = GMT_F32;
+    p->scheme = GMT_SCHEME_UNSPLIT;
+    p->recon = GMT_RECON_MC;
+    p->riemann = GMT_RIEMANN_HLLD;
+    p->iflo = 1;
+    p->emf = GMT_EMF_AVERAGE;
+    p->boxlen = 1.0;
+    p->gamma = 1.01;
+    p->courant = 0.7;
+    p->smallr = 1e-6;
+    p->smallc = 1e-4;
+    p->smallp = 1e-6;
+    p->glm_ch_scale = 0.25;
+    p->glm_cp_coef = 0.18;
+    p->turb_min_rho = 1e-5;
+    p->turb_amp = 0.0;
+    p->turb_T = 0.3;
+    p->turb_ndt = 100;
+    p->turb_seed = 1;
+    return GMT_OK;
+}
+
+int gmt_create(const gmt_params* p, gmt_ctx** out) {
+    if (!p || !out) return fail(GMT_ERR_ARG, "gmt_create: null argument");
+    *out = nullptr;
+    if (p->abi_version != GMT_ABI_VERSION) return fail(GMT_ERR_ARG, "gmt_create: abi_version mismatch");
+    if (p->nx < 1 || p->ny < 1 || p->nz < 1) return fail(GMT_ERR_ARG, "gmt_create: grid dimensions must be >= 1");
+    if ((double)p->nx * p->ny * p->nz > 4.0e9) return fail(GMT_ERR_ARG, "gmt_create: grid too large (> 4e9 cells)");
+    if (p->dtype != GMT_F32 && p->dtype != GMT_F64) return fail(GMT_ERR_ARG, "gmt_create: dtype must be GMT_F32 or GMT_F64");
+    if (p->scheme < 0 || p->scheme > 2) return fail(GMT_ERR_ARG, "gmt_create: unknown scheme");
+    if (p->recon < 0 || p->recon > 2) return fail(GMT_ERR_ARG, "gmt_create: unknown recon");
+    if (p->riemann < 0 || p->riemann > 3) return fail(GMT_ERR_ARG, "gmt_create: unknown riemann");
+    if (p->scheme == GMT_SCHEME_MARCH1D && p->riemann != GMT_RIEMANN_HLL)
+        return fail(GMT_ERR_UNSUPPORTED, "gmt_create: the march scheme uses HLL (spike_mhd.cu:199-223)");
+    if (p->scheme == GMT_SCHEME_CT && p->riemann != GMT_RIEMANN_HLL && p->riemann != GMT_RIEMANN_HLLD)
+        return fail(GMT_ERR_UNSUPPORTED, "gmt_create: CT supports HLL and HLLD");
+    if (!(p->gamma > 1.0) || !(p->boxlen > 0.0) || !(p->smallr > 0.0))
+        return fail(GMT_ERR_ARG, "gmt_create: gamma > 1, boxlen > 0 and smallr > 0 are required");
+    if (p->scheme == GMT_SCHEME_CT && p->recon == GMT_RECON_MINMOD)
+        return fail(GMT_ERR_UNSUPPORTED, "gmt_create: CT supports MC and PPM reconstruction");
+    std::call_once(g_mode_once, [] { g_mode_err = upload_mode_table(); });
+    if (g_mode_err != cudaSuccess) return cuda_fail(g_mode_err, "mode table");
+
+    gmt_ctx* c = new gmt_ctx();
+    c->p = *p;
+    c->esize = p->dtype == GMT_F64 ? 8 : 4;
+    c->n = (size_t)p->nx * p->ny * p->nz;
+    cudaGetDevice(&c->device);
+    int rc = GMT_OK;
+    if (p->scheme == GMT_SCHEME_UNSPLIT) rc = choose_tile(c);
+    if (rc != GMT_OK) { delete c; return rc; }
+    auto alloc = [&](void** ptr, size_t bytes) -> bool {
+        cudaError_t e = cudaMalloc(ptr, bytes);
+        if (e != cudaSuccess) { cuda_fail(e, "cudaMalloc"); return false; }
+        return true;
+    };
+    bool ok = alloc((void**)&c->cfl, 4 * sizeof(unsigned long long)) &&
+              alloc((void**)&c->diag_part, (size_t)c->diag_blocks * 8 * sizeof(double)) &&
+              alloc((void**)&c->diag_out, 16 * sizeof(double)) &&
+              alloc((void**)&c->modes, NMODES * 6 * sizeof(double)) &&
+              alloc(&c->btab, (size_t)p->ny * p->nz * 24 * c->esize);
+    const int dims[3] = {p->nx, p->ny, p->nz};
+    for (int a = 0; ok && a < 3; ++a) ok = alloc(&c->trig[a], (size_t)8 * dims[a] * c->esize);
+    if (ok && p->scheme == GMT_SCHEME_CT) ok = alloc(&c->ct_scratch, (size_t)27 * c->n * c->esize);
+    if (ok) ok = alloc((void**)&c->divb, sizeof(unsigned long long));
+    if (!ok) { gmt_destroy(c); return GMT_ERR_NOMEM; }
+    for (int a = 0; a < 3; ++a) {
+        std::vector<double> t = trig_table(dims[a]);
+        cudaError_t e;
+        if (c->esize == 8) {
+            e = cudaMemcpy(c->trig[a], t.data(), t.size() * 8, cudaMemcpyHostToDevice);
+        } else {
+            std::vector<float> f(t.begin(), t.end());
+            e = cudaMemcpy(c->trig[a], f.data(), f.size() * 4, cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) { gmt_destroy(c); return cuda_fail(e, "trig upload"); }
+    }
+    int nd = p->turb_ndt > 0 ? p->turb_ndt : 100;
+    double dtf = p->turb_T / nd;
+    c->alpha = 1.0 - dtf / p->turb_T;
+    c->beta = std::sqrt(2.0 * dtf / p->turb_T);
+    c->sigma0 = forcing_sigma0(p->turb_amp, c->alpha, c->beta);
+    rc = gmt_forcing_reset(c, nullptr);
+    if (rc == GMT_OK) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) rc = cuda_fail(e, "gmt_create");
+    }
+    if (rc != GMT_OK) { gmt_destroy(c); return rc; }
+    *out = c;
+    return GMT_OK;
+}
+
+int gmt_destroy(gmt_ctx* c) {
+    if (!c) return GMT_OK;
+    cudaFree(c->cfl);
+    cudaFree(c->diag_part);
+    cudaFree(c->diag_out);
+    cudaFree(c->modes);
+    cudaFree(c->btab);
+    for (auto& t : c->trig) cudaFree(t);
+    cudaFree(c->ct_scratch);
+    cudaFree(c->divb);
+    delete c;
+    return GMT_OK;
+}
+
+int gmt_kernel_info(gmt_ctx* c, int32_t* regs, int64_t* smem, int32_t tile[3]) {
+    if (!c) return fail(GMT_ERR_ARG, "null context");
+    int r = -1;
+    int64_t sm = 0;
+    if (c->p.scheme == GMT_SCHEME_UNSPLIT) {
+        r = unsplit_regs(c->esize, c->p.recon, c->p.riemann == GMT_RIEMANN_LLF ? GMT_RIEMANN_HLLD : c->p.riemann);
+        sm = (int64_t)unsplit_smem(c->esize, c->ox, c->oy);
+    } else if (c->p.scheme == GMT_SCHEME_MARCH1D) {
+        r = march1d_regs(c->esize);
+    } else {
+        r = ct_regs_of(c->esize);
+        sm = (int64_t)ct_smem_of(c->esize, c->ox, c->oy);
+    }
+    if (regs) *regs = r;
+    if (smem) *smem = sm;
+    if (tile) { tile[0] = c->ox; tile[1] = c->oy; tile[2] = c->lz; }
+    return GMT_OK;
+}
+
+int gmt_step(gmt_ctx* c, const void* uold, void* unew, const gmt_step_args* a, void* stream) {
+    if (!c || !uold || !unew || !a) return fail(GMT_ERR_ARG, "gmt_step: null argument");
+    if (uold == unew) return fail(GMT_ERR_ARG, "gmt_step: uold and unew must be different buffers");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (c->esize == 8) return step_impl<double>(c, cplanes<double>(uold, c->n), planes<double>(unew, c->n), a, s);
+    return step_impl<float>(c, cplanes<float>(uold, c->n), planes<float>(unew, c->n), a, s);
+}
+
+int gmt_step_planes(gmt_ctx* c, const void* const* uold, void* const* unew, const gmt_step_args* a, void* stream) {
+    if (!c || !uold || !unew || !a) return fail(GMT_ERR_ARG, "gmt_step_planes: null argument");
+    for (int v = 0; v < 9; ++v)
+        if (!uold[v] || !unew[v]) return fail(GMT_ERR_ARG, "gmt_step_planes: null plane pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (c->esize == 8) {
+        CPlanes<double> u; Planes<double> o;
+        for (int v = 0; v < 9; ++v) { u.p[v] = (const double*)uold[v]; o.p[v] = (double*)unew[v]; }
+        return step_impl<double>(c, u, o, a, s);
+    }
+    CPlanes<float> u; Planes<float> o;
+    for (int v = 0; v < 9; ++v) { u.p[v] = (const float*)uold[v]; o.p[v] = (float*)unew[v]; }
+    return step_impl<float>(c, u, o, a, s);
+}
+
+int gmt_cfl_async(gmt_ctx* c, const void* u, void* stream) {
+    if (!c || !u) return fail(GMT_ERR_ARG, "gmt_cfl_async: null argument");
+    if (c->p.scheme == GMT_SCHEME_CT) return gmt_ct_cfl_async(c, u, stream);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = c->esize == 8 ? launch_cfl<double>(cplanes<double>(u, c->n), c->n, consts_of<double>(c->p), c->cfl, s)
+                                  : launch_cfl<float>(cplanes<float>(u, c->n), c->n, consts_of<float>(c->p), c->cfl, s);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "cfl");
+}
+
+int gmt_cfl_result(gmt_ctx* c, double out[2], void* stream) {
+    if (!c || !out) return fail(GMT_ERR_ARG, "gmt_cfl_result: null argument");
+    unsigned long long h[2];
+    GMT_CUDA(cudaMemcpyAsync(h, c->cfl, sizeof(h), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    GMT_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    std::memcpy(&out[0], &h[0], 8);
+    std::memcpy(&out[1], &h[1], 8);
+    if (!std::isfinite(out[0]) || !(out[0] > 0.0)) return fail(GMT_ERR_STATE, "CFL maximum is not positive and finite");
+    return GMT_OK;
+}
+
+int gmt_compute_dt(gmt_ctx* c, const void* u, double* dt, void* stream) {
+    if (!dt) return fail(GMT_ERR_ARG, "gmt_compute_dt: null dt");
+    int rc = gmt_cfl_async(c, u, stream);
+    if (rc) return rc;
+    double m[2];
+    rc = gmt_cfl_result(c, m, stream);
+    if (rc) return rc;
+    *dt = c->p.courant * (c->p.boxlen / c->p.nx) / m[0];
+    return GMT_OK;
+}
+
+int gmt_diagnostics(gmt_ctx* c, const void* u, gmt_diag* out, void* stream) {
+    if (!c || !u || !out) return fail(GMT_ERR_ARG, "gmt_diagnostics: null argument");
+    if (c->p.scheme == GMT_SCHEME_CT) return fail(GMT_ERR_ARG, "gmt_diagnostics: GLM state only; use gmt_ct_divb_max");
+    cudaStream_t s = (cudaStream_t)stream;
+    const double dx = c->p.boxlen / c->p.nx;
+    cudaError_t e = c->esize == 8
+                        ? launch_diag<double>(cplanes<double>(u, c->n), c->p.nx, c->p.ny, c->p.nz, dx, c->p.smallr,
+                                              c->diag_part, c->diag_blocks, c->diag_out, s)
+                        : launch_diag<float>(cplanes<float>(u, c->n), c->p.nx, c->p.ny, c->p.nz, dx, c->p.smallr,
+                                             c->diag_part, c->diag_blocks, c->diag_out, s);
+    if (e != cudaSuccess) return cuda_fail(e, "diagnostics");
+    double h[8];
+    GMT_CUDA(cudaMemcpyAsync(h, c->diag_out, sizeof(h), cudaMemcpyDeviceToHost, s));
+    GMT_CUDA(cudaStreamSynchronize(s));
+    out->mass = h[0]; out->ke2 = h[1]; out->etot = h[2];
+    out->psi_l2 = std::sqrt(h[3] / (double)c->n);
+    out->divb_l2 = std::sqrt(h[4] / (double)c->n);
+    out->divbmax = h[5]; out->rhomin = h[6];
+    out->vrms = std::sqrt(h[1] / h[0]);
+    out->nonfinite_cells = (int32_t)h[7];
+    out->finite = h[7] == 0.0;
+    return GMT_OK;
+}
+
+int gmt_forcing_reset(gmt_ctx* c, void* stream) {
+    if (!c) return fail(GMT_ERR_ARG, "null context");
+    cudaStream_t s = (cudaStream_t)stream;
+    GMT_CUDA(cudaMemsetAsync(c->modes, 0, NMODES * 6 * sizeof(double), s));
+    c->counter = 0;
+    return refresh_btab_any(c, s);
+}
+
+int gmt_forcing_advance(gmt_ctx* c, void* stream) {
+    if (!c) return fail(GMT_ERR_ARG, "null context");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = launch_ou_update(c->modes, c->p.turb_seed, c->counter, c->alpha, c->beta, c->sigma0, s);
+    if (e != cudaSuccess) return cuda_fail(e, "OU update");
+    c->counter++;
+    return refresh_btab_any(c, s);
+}
+
+int gmt_forcing_set_modes(gmt_ctx* c, const double* modes, void* stream) {
+    if (!c || !modes) return fail(GMT_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    GMT_CUDA(cudaMemcpyAsync(c->modes, modes, NMODES * 6 * sizeof(double), cudaMemcpyHostToDevice, s));
+    GMT_CUDA(cudaStreamSynchronize(s));
+    return refresh_btab_any(c, s);
+}
+
+int gmt_forcing_get_modes(gmt_ctx* c, double* modes, void* stream) {
+    if (!c || !modes) return fail(GMT_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    GMT_CUDA(cudaMemcpyAsync(modes, c->modes, NMODES * 6 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GMT_CUDA(cudaStreamSynchronize(s));
+    return GMT_OK;
+}
+
+int gmt_forcing_counter(gmt_ctx* c, uint32_t* counter) {
+    if (!c || !counter) return fail(GMT_ERR_ARG, "null argument");
+    *counter = c->counter;
+    return GMT_OK;
+}
+
+int gmt_ic_orszag_tang(gmt_ctx* c, void* u, void* stream) {
+    if (!c || !u) return fail(GMT_ERR_ARG, "null argument");
+    if (c->p.scheme == GMT_SCHEME_CT) return gmt_ct_ic_orszag_tang(c, u, stream);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = c->esize == 8 ? launch_ic_ot<double>(planes<double>(u, c->n), c->p.nx, c->p.ny, c->p.nz, c->p.gamma, s)
+                                  : launch_ic_ot<float>(planes<float>(u, c->n), c->p.nx, c->p.ny, c->p.nz, c->p.gamma, s);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "ic");
+}
+
+int gmt_ic_uniform(gmt_ctx* c, void* u, double rho0, double p0, double bx0, double by0, double bz0, void* stream) {
+    if (!c || !u) return fail(GMT_ERR_ARG, "null argument");
+    if (c->p.scheme == GMT_SCHEME_CT) return fail(GMT_ERR_ARG, "gmt_ic_uniform: GLM state only");
+    double v9[9] = {rho0, 0, 0, 0, p0 / (c->p.gamma - 1.0) + 0.5 * (bx0 * bx0 + by0 * by0 + bz0 * bz0), bx0, by0, bz0, 0};
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = c->esize == 8 ? launch_ic_uniform<double>(planes<double>(u, c->n), c->n, v9, s)
+                                  : launch_ic_uniform<float>(planes<float>(u, c->n), c->n, v9, s);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "ic");
+}
+
+int gmt_ic_turbulent(gmt_ctx* c, void* u, double rho0, double p0, double bx0, double by0, double bz0, double mach,
+                     double db, uint32_t seed, void* stream) {
+    if (!c || !u) return fail(GMT_ERR_ARG, "null argument");
+    if (c->p.scheme == GMT_SCHEME_CT) return fail(GMT_ERR_ARG, "gmt_ic_turbulent: GLM state only");
+    if (!(rho0 > 0) || !(p0 > 0)) return fail(GMT_ERR_ARG, "gmt_ic_turbulent: rho0 and p0 must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    double* m = nullptr;
+    void* bt = nullptr;
+    GMT_CUDA(cudaMalloc(&m, NMODES * 6 * sizeof(double)));
+    cudaError_t e = cudaMalloc(&bt, (size_t)c->p.ny * c->p.nz * 24 * c->esize);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m, 0, NMODES * 6 * sizeof(double), s);
+    if (e == cudaSuccess) e = launch_ou_update(m, seed, 0u, 0.0, 1.0, forcing_sigma0(1.0, 0.0, 1.0), s);
+    const double b0[3] = {bx0, by0, bz0};
+    const double vscale = mach * std::sqrt(c->p.gamma * p0 / rho0);
+    if (e == cudaSuccess) {
+        if (c->esize == 8) {
+            e = launch_btab<double>(m, (const double*)c->trig[1], (const double*)c->trig[2], c->p.ny, c->p.nz,
+                                    (double*)bt, s);
+            if (e == cudaSuccess)
+                e = launch_ic_turb<double>(planes<double>(u, c->n), c->p.nx, c->p.ny, c->p.nz, (const double*)bt,
+                                           (const double*)c->trig[0], rho0, p0, b0, vscale, db, c->p.gamma, s);
+        } else {
+            e = launch_btab<float>(m, (const float*)c->trig[1], (const float*)c->trig[2], c->p.ny, c->p.nz,
+                                   (float*)bt, s);
+            if (e == cudaSuccess)
+                e = launch_ic_turb<float>(planes<float>(u, c->n), c->p.nx, c->p.ny, c->p.nz, (const float*)bt,
+                                          (const float*)c->trig[0], rho0, p0, b0, vscale, db, c->p.gamma, s);
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(m);
+    cudaFree(bt);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_ic_turbulent");
+}
+
+// ------------------------------------------------------------------------------------------
+// CT
+// ------------------------------------------------------------------------------------------
+int gmt_ct_step(gmt_ctx* c, const void* qold, void* qnew, const gmt_step_args* a, void* stream) {
+    if (!c || !qold || !qnew || !a) return fail(GMT_ERR_ARG, "gmt_ct_step: null argument");
+    if (c->p.scheme != GMT_SCHEME_CT) return fail(GMT_ERR_ARG, "gmt_ct_step: context scheme is not GMT_SCHEME_CT");
+    if (qold == qnew) return fail(GMT_ERR_ARG, "gmt_ct_step: qold and qnew must be different buffers");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (c->esize == 8) return ct_step_impl<double>(c, cplanes8<double>(qold, c->n), planes8<double>(qnew, c->n), a, s);
+    return ct_step_impl<float>(c, cplanes8<float>(qold, c->n), planes8<float>(qnew, c->n), a, s);
+}
+
+int gmt_ct_cfl_async(gmt_ctx* c, const void* q, void* stream) {
+    if (!c || !q) return fail(GMT_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = c->esize == 8
+                        ? launch_ct_cfl<double>(cplanes8<double>(q, c->n), c->p.nx, c->p.ny, c->p.nz,
+                                                consts_of<double>(c->p), c->cfl, s)
+                        : launch_ct_cfl<float>(cplanes8<float>(q, c->n), c->p.nx, c->p.ny, c->p.nz,
+                                               consts_of<float>(c->p), c->cfl, s);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "ct cfl");
+}
+
+int gmt_ct_divb_max(gmt_ctx* c, const void* q, double* out, void* stream) {
+    if (!c || !q || !out) return fail(GMT_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const double dx = c->p.boxlen / c->p.nx;
+    cudaError_t e = c->esize == 8
+                        ? launch_ct_divb<double>(cplanes8<double>(q, c->n), c->p.nx, c->p.ny, c->p.nz, dx, c->divb, s)
+                        : launch_ct_divb<float>(cplanes8<float>(q, c->n), c->p.nx, c->p.ny, c->p.nz, dx, c->divb, s);
+    if (e != cudaSuccess) return cuda_fail(e, "divb");
+    unsigned long long h;
+    GMT_CUDA(cudaMemcpyAsync(&h, c->divb, 8, cudaMemcpyDeviceToHost, s));
+    GMT_CUDA(cudaStreamSynchronize(s));
+    std::memcpy(out, &h, 8);
+    return GMT_OK;
+}
+
+int gmt_ct_ic_orszag_tang(gmt_ctx* c, void* q, void* stream) {
+    if (!c || !q) return fail(GMT_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = c->esize == 8 ? launch_ct_ic_ot<double>(planes8<double>(q, c->n), c->p.nx, c->p.ny, c->p.nz, c->p.gamma, s)
+                                  : launch_ct_ic_ot<float>(planes8<float>(q, c->n), c->p.nx, c->p.ny, c->p.nz, c->p.gamma, s);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "ct ic");
+}
+
+// ------------------------------------------------------------------------------------------
+// legacy bridge ABI: __constant__-style setters become process-wide state (spike_mhd.cu:52,
+// 321-340); each grid size gets its own lazily created FP32 context.
+// ------------------------------------------------------------------------------------------
+#ifndef GMT_LEGACY_NX
+#define GMT_LEGACY_NX 480
+#endif
+static std::mutex g_legacy_mu;
+static int g_legacy_nx = GMT_LEGACY_NX;
+static float g_dtdx = 0.02f, g_ch = 1.0f, g_glmfac = 1.0f, g_gamma = 1.4f;
+static gmt_ctx* g_legacy_ctx[2] = {nullptr, nullptr};   // [0] march, [1] CT
+static float g_legacy_gamma_of[2] = {0.f, 0.f};
+
+static gmt_ctx* legacy_ctx(int which) {
+    gmt_ctx*& c = g_legacy_ctx[which];
+    if (c && (c->p.nx != g_legacy_nx || g_legacy_gamma_of[which] != g_gamma)) { gmt_destroy(c); c = nullptr; }
+    if (!c) {
+        gmt_params p;
+        gmt_params_init(&p, g_legacy_nx);
+        p.scheme = which == 0 ? GMT_SCHEME_MARCH1D : GMT_SCHEME_CT;
+        p.riemann = GMT_RIEMANN_HLL;
+        p.gamma = g_gamma;
+        p.smallr = 1e-6;
+        p.smallp = 1e-6;
+        p.boxlen = 1.0;
+        if (gmt_create(&p, &c) != GMT_OK) c = nullptr;
+        g_legacy_gamma_of[which] = g_gamma;
+    }
+    return c;
+}
+
+int march_nv(void) { return 9; }
+int march_nx(void) { return g_legacy_nx; }
+int march_nsp(void) { return 0; }
+void march_set_nx(int n) {
+    std::lock_guard<std::mutex> lk(g_legacy_mu);
+    if (n > 0) g_legacy_nx = n;
+}
+void march_set_dtdx(float v) { g_dtdx = v; }
+void march_set_glm(float ch, float fac) { g_ch = ch; g_glmfac = fac; }
+void march_set_gamma(float g) { g_gamma = g; }
+
+double march_run_dev(float* const* qv, float* const* ov, int nsteps) {
+    std::lock_guard<std::mutex> lk(g_legacy_mu);
+    gmt_ctx* c = legacy_ctx(0);
+    if (!c || !qv || !ov || nsteps < 0) return -1.0;
+    const double dx = c->p.boxlen / c->p.nx;
+    gmt_step_args a{};
+    a.dt = (double)g_dtdx * dx;
+    a.ch = g_ch;
+    a.glm_fac = g_glmfac;
+    const void* q[9];
+    void* o[9];
+    for (int v = 0; v < 9; ++v) { q[v] = qv[v]; o[v] = ov[v]; }
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0);
+    bool in_q = true;
+    for (int it = 0; it < nsteps; ++it) {
+        if (gmt_step_planes(c, in_q ? q : (const void* const*)o, in_q ? o : (void* const*)q, &a, nullptr) != GMT_OK) break;
+        in_q = !in_q;
+    }
+    cudaEventRecord(t1);
+    cudaEventSynchronize(t1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (!in_q)
+        for (int v = 0; v < 9; ++v) cudaMemcpy(qv[v], ov[v], c->n * sizeof(float), cudaMemcpyDeviceToDevice);
+    return (double)ms;
+}
+
+double ct_run(float* const* qv, float* const* ov, float* const* cc, int nsteps) {
+    (void)cc;  // the face-averaged field is formed inside the kernels; the scratch planes are unused
+    std::lock_guard<std::mutex> lk(g_legacy_mu);
+    gmt_ctx* c = legacy_ctx(1);
+    if (!c || !qv || !ov || nsteps < 0) return -1.0;
+    const double dx = c->p.boxlen / c->p.nx;
+    gmt_step_args a{};
+    a.dt = (double)g_dtdx * dx;
+    CPlanes8<float> q, o;
+    Planes8<float> qw, ow;
+    for (int v = 0; v < 8; ++v) { q.p[v] = qv[v]; o.p[v] = ov[v]; qw.p[v] = qv[v]; ow.p[v] = ov[v]; }
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0);
+    bool in_q = true;
+    for (int it = 0; it < nsteps; ++it) {
+        int rc = in_q ? ct_step_impl<float>(c, q, ow, &a, nullptr) : ct_step_impl<float>(c, o, qw, &a, nullptr);
+        if (rc != GMT_OK) break;
+        in_q = !in_q;
+    }
+    cudaEventRecord(t1);
+    cudaEventSynchronize(t1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (!in_q)
+        for (int v = 0; v < 8; ++v) cudaMemcpy(qv[v], ov[v], c->n * sizeof(float), cudaMemcpyDeviceToDevice);
+    return (double)ms;
+}
+
+int ct_regs(void) { return ct_regs_of(4); }
+int ct_shmem(void) { return (int)ct_smem_of(4, 0, 0); }
+
+}  // extern "C"
+
+namespace gmt {
+int unsplit_regs_f32(int recon, int riem);
+int unsplit_regs_f64(int recon, int riem);
+int unsplit_regs(int esize, int recon, int riem) {
+    return esize == 8 ? unsplit_regs_f64(recon, riem) : unsplit_regs_f32(recon, riem);
+}
+int unsplit_max_threads(int) { return 256; }
+size_t unsplit_smem(int esize, int ox, int oy) {
+    return esize == 8 ? unsplit_smem_bytes<double>(ox, oy) : unsplit_smem_bytes<float>(ox, oy);
+}
+}  // namespace gmt

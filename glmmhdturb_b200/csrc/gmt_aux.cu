@@ -1,0 +1,444 @@
+// gmt_aux.cu -- CFL reduction, diagnostics, OU mode forcing, initial conditions.
+//
+// CFL: ctot = sum_d(|v_d| + c_f(B_d)) per cell, dt = courant*dx/max(ctot) (glmmhd_turb.jl:1963-1978),
+// reduced in FP64 with a warp-shuffle max and one atomic per block.
+// Diagnostics (glmmhd_turb.jl:1996-2018): FP64 sums over a fixed grid and a fixed tree, so the
+// result does not depend on scheduling.
+// Forcing: the 61 +/- mode pairs with 1 <= |k|^2 <= 9 advance by an OU step driven by
+// Philox4x32-10 normals (solenoidal projection as glmmhd_turb.jl:2104-2108 with comp_frac = 0);
+// the per-row table B[kx][c] = sum_{modes with kx} ahat_c e^{i(ky y + kz z)} turns the step
+// kernel's mode sum into 4 complex multiply-adds per component.
+#include <cstdio>
+
+#include "gmt_internal.h"
+
+namespace gmt {
+
+__constant__ int c_mode_k[NMODES * 3];
+
+// ------------------------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(256) cfl_kernel(const CPlanes<R> u, size_t n, const Consts<R> K,
+                                                  unsigned long long* out) {
+    __shared__ double red[32];
+    double cm = 0.0, sm = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        Q9<R> c;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) c.v[v] = u.p[v][i];
+        R ct, sg;
+        cfl_speeds(c, K, ct, sg);
+        cm = fmax(cm, (double)ct);
+        sm = fmax(sm, (double)sg);
+    }
+    block_max_atomic(cm, out, red);
+    __syncthreads();
+    block_max_atomic(sm, out + 1, red);
+}
+
+template <class R>
+cudaError_t launch_cfl(const CPlanes<R>& u, size_t n, const Consts<R>& K, unsigned long long* out, cudaStream_t s) {
+    int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+    cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), s);
+    cfl_kernel<R><<<nb, 256, 0, s>>>(u, n, K, out);
+    return cudaGetLastError();
+}
+
+// CT: cell prims from the face-averaged field
+template <class R>
+__global__ void __launch_bounds__(256) ct_cfl_kernel(const CPlanes8<R> qv, int nx, int ny, int nz, const Consts<R> K,
+                                                     unsigned long long* out) {
+    __shared__ double red[32];
+    const R* const* q = qv.p;
+    size_t n = (size_t)nx * ny * nz;
+    double cm = 0.0, sm = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        size_t ixp = (size_t)wrapi(x + 1, nx) + (size_t)nx * (y + (size_t)ny * z);
+        size_t iyp = (size_t)x + (size_t)nx * (wrapi(y + 1, ny) + (size_t)ny * z);
+        size_t izp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrapi(z + 1, nz));
+        Q9<R> c;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) c.v[v] = q[v][i];
+        c.v[5] = R(0.5) * (q[5][i] + q[5][ixp]);
+        c.v[6] = R(0.5) * (q[6][i] + q[6][iyp]);
+        c.v[7] = R(0.5) * (q[7][i] + q[7][izp]);
+        c.v[8] = R(0);
+        R ct, sg;
+        cfl_speeds(c, K, ct, sg);
+        cm = fmax(cm, (double)ct);
+        sm = fmax(sm, (double)sg);
+    }
+    block_max_atomic(cm, out, red);
+    __syncthreads();
+    block_max_atomic(sm, out + 1, red);
+}
+
+template <class R>
+cudaError_t launch_ct_cfl(const CPlanes8<R>& q, int nx, int ny, int nz, const Consts<R>& K, unsigned long long* out,
+                          cudaStream_t s) {
+    size_t n = (size_t)nx * ny * nz;
+    int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+    cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), s);
+    ct_cfl_kernel<R><<<nb, 256, 0, s>>>(q, nx, ny, nz, K, out);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// diagnostics: 8 quantities per block, then a single-block fixed-order reduction
+// ------------------------------------------------------------------------------------------
+constexpr int NDIAG = 8;  // mass, ke2, etot, psi2, divb2, divbmax, rhomin, nonfinite
+
+__device__ __forceinline__ void diag_combine(double* a, const double* b) {
+    for (int k = 0; k < 5; ++k) a[k] += b[k];
+    a[5] = fmax(a[5], b[5]);
+    a[6] = fmin(a[6], b[6]);
+    a[7] += b[7];
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) diag_kernel(const CPlanes<R> u, int nx, int ny, int nz, double dx, double smallr,
+                                                   double* partials) {
+    __shared__ double sh[256 * NDIAG];
+    double acc[NDIAG] = {0, 0, 0, 0, 0, 0, 1e300, 0};
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        double rho = (double)u.p[0][i], mx = (double)u.p[1][i], my = (double)u.p[2][i], mz = (double)u.p[3][i];
+        double ps = (double)u.p[8][i];
+        acc[0] += rho;
+        acc[1] += (mx * mx + my * my + mz * mz) / fmax(rho, smallr);
+        acc[2] += (double)u.p[4][i];
+        acc[3] += ps * ps;
+        auto at = [&](int a, int b, int c) {
+            return (size_t)wrapi(a, nx) + (size_t)nx * ((size_t)wrapi(b, ny) + (size_t)ny * wrapi(c, nz));
+        };
+        double bxp = u.p[5][at(x + 1, y, z)], bxm = u.p[5][at(x - 1, y, z)];
+        double byp = u.p[6][at(x, y + 1, z)], bym = u.p[6][at(x, y - 1, z)];
+        double bzp = u.p[7][at(x, y, z + 1)], bzm = u.p[7][at(x, y, z - 1)];
+        double db = fabs((bxp - bxm) + (byp - bym) + (bzp - bzm)) / (2.0 * dx);
+        acc[4] += db * db;
+        acc[5] = fmax(acc[5], db);
+        acc[6] = fmin(acc[6], rho);
+        bool fin = true;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) fin = fin && isfinite((double)u.p[v][i]);
+        acc[7] += fin ? 0.0 : 1.0;
+    }
+    for (int k = 0; k < NDIAG; ++k) sh[threadIdx.x * NDIAG + k] = acc[k];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) diag_combine(&sh[threadIdx.x * NDIAG], &sh[(threadIdx.x + s) * NDIAG]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NDIAG; ++k) partials[blockIdx.x * NDIAG + k] = sh[k];
+}
+
+__global__ void __launch_bounds__(256) diag_final(const double* partials, int nb, double* out) {
+    __shared__ double sh[256 * NDIAG];
+    double acc[NDIAG] = {0, 0, 0, 0, 0, 0, 1e300, 0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) diag_combine(acc, partials + b * NDIAG);
+    for (int k = 0; k < NDIAG; ++k) sh[threadIdx.x * NDIAG + k] = acc[k];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) diag_combine(&sh[threadIdx.x * NDIAG], &sh[(threadIdx.x + s) * NDIAG]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NDIAG; ++k) out[k] = sh[k];
+}
+
+template <class R>
+cudaError_t launch_diag(const CPlanes<R>& u, int nx, int ny, int nz, double dx, double smallr, double* partials,
+                        int nblocks, double* out, cudaStream_t s) {
+    diag_kernel<R><<<nblocks, 256, 0, s>>>(u, nx, ny, nz, dx, smallr, partials);
+    diag_final<<<1, 256, 0, s>>>(partials, nblocks, out);
+    return cudaGetLastError();
+}
+
+// CT face div B max: (upper - lower)/dx per dim (ct_mhd.jl:190-194)
+template <class R>
+__global__ void __launch_bounds__(256) ct_divb_kernel(const CPlanes8<R> qv, int nx, int ny, int nz, double dx,
+                                                      unsigned long long* out) {
+    __shared__ double red[32];
+    const R* bx = qv.p[5];
+    const R* by = qv.p[6];
+    const R* bz = qv.p[7];
+    size_t n = (size_t)nx * ny * nz;
+    double m = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        size_t ixp = (size_t)wrapi(x + 1, nx) + (size_t)nx * (y + (size_t)ny * z);
+        size_t iyp = (size_t)x + (size_t)nx * (wrapi(y + 1, ny) + (size_t)ny * z);
+        size_t izp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrapi(z + 1, nz));
+        double d = ((double)bx[ixp] - (double)bx[i] + (double)by[iyp] - (double)by[i] + (double)bz[izp] -
+                    (double)bz[i]) / dx;
+        m = fmax(m, fabs(d));
+    }
+    block_max_atomic(m, out, red);
+}
+
+template <class R>
+cudaError_t launch_ct_divb(const CPlanes8<R>& q, int nx, int ny, int nz, double dx, unsigned long long* out,
+                           cudaStream_t s) {
+    size_t n = (size_t)nx * ny * nz;
+    int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+    cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
+    ct_divb_kernel<R><<<nb, 256, 0, s>>>(q, nx, ny, nz, dx, out);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// forcing
+// ------------------------------------------------------------------------------------------
+cudaError_t upload_mode_table() {
+    int k[NMODES * 3];
+    int n = 0;
+    for (int kx = 0; kx <= 3; ++kx)
+        for (int ky = -3; ky <= 3; ++ky)
+            for (int kz = -3; kz <= 3; ++kz) {
+                int k2 = kx * kx + ky * ky + kz * kz;
+                if (k2 < 1 || k2 > 9) continue;
+                bool half = kx > 0 || (kx == 0 && ky > 0) || (kx == 0 && ky == 0 && kz > 0);
+                if (!half) continue;
+                if (n < NMODES) { k[3 * n] = kx; k[3 * n + 1] = ky; k[3 * n + 2] = kz; }
+                ++n;
+            }
+    if (n != NMODES) return cudaErrorInvalidValue;
+    return cudaMemcpyToSymbol(c_mode_k, k, sizeof(k));
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11)
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+
+__global__ void ou_update_kernel(double* modes, uint32_t seed, uint32_t counter, double alpha, double beta,
+                                 double sigma0) {
+    int q = threadIdx.x;
+    if (q >= NMODES) return;
+    uint32_t r[8] = {counter, (uint32_t)q, 0u, 0u, counter, (uint32_t)q, 1u, 0u};
+    philox4x32_10(r, seed, 0x9E3779B9u);
+    philox4x32_10(r + 4, seed, 0x9E3779B9u);
+    const double twopi = 6.283185307179586476925286766559;
+    double z[6];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        double u1 = ((double)r[2 * b] + 0.5) * 2.3283064365386962890625e-10;
+        double u2 = ((double)r[2 * b + 1] + 0.5) * 2.3283064365386962890625e-10;
+        double rr = sqrt(-2.0 * log(u1));
+        double th = twopi * u2;
+        z[2 * b] = rr * cos(th);
+        z[2 * b + 1] = rr * sin(th);
+    }
+    double kx = c_mode_k[3 * q], ky = c_mode_k[3 * q + 1], kz = c_mode_k[3 * q + 2];
+    double kk = sqrt(kx * kx + ky * ky + kz * kz);
+    double ux = kx / kk, uy = ky / kk, uz = kz / kk;
+    double sig = sigma0 / kk;
+    double kr = ux * z[0] + uy * z[2] + uz * z[4];
+    double ki = ux * z[1] + uy * z[3] + uz * z[5];
+    double uu[3] = {ux, uy, uz};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double pr = z[2 * c] - uu[c] * kr;
+        double pi = z[2 * c + 1] - uu[c] * ki;
+        double* m = modes + (q * 3 + c) * 2;
+        m[0] = alpha * m[0] + beta * sig * pr;
+        m[1] = alpha * m[1] + beta * sig * pi;
+    }
+}
+
+cudaError_t launch_ou_update(double* modes, uint32_t seed, uint32_t counter, double alpha, double beta, double sigma0,
+                             cudaStream_t s) {
+    ou_update_kernel<<<1, 64, 0, s>>>(modes, seed, counter, alpha, beta, sigma0);
+    return cudaGetLastError();
+}
+
+// B[kx][c] per (y,z) row, same summation order as the oracle's Forcer::accel
+template <class R>
+__global__ void __launch_bounds__(256) btab_kernel(const double* modes, const R* trigy, const R* trigz, int ny, int nz,
+                                                   R* btab) {
+    int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= ny * nz) return;
+    int j = row % ny, k = row / ny;
+    R* out = btab + (size_t)row * 24;
+    int q = 0;
+    for (int kx = 0; kx <= 3; ++kx) {
+        R Br[3] = {R(0), R(0), R(0)}, Bi[3] = {R(0), R(0), R(0)};
+        while (q < NMODES && c_mode_k[3 * q] == kx) {
+            int ky = c_mode_k[3 * q + 1], kz = c_mode_k[3 * q + 2];
+            int ay = ky < 0 ? -ky : ky, az = kz < 0 ? -kz : kz;
+            R eyr = trigy[(2 * ay) * ny + j], eyi = trigy[(2 * ay + 1) * ny + j];
+            R ezr = trigz[(2 * az) * nz + k], ezi = trigz[(2 * az + 1) * nz + k];
+            if (ky < 0) eyi = -eyi;
+            if (kz < 0) ezi = -ezi;
+            R er = eyr * ezr - eyi * ezi;
+            R ei = eyr * ezi + eyi * ezr;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R ar = (R)modes[(q * 3 + c) * 2], ai = (R)modes[(q * 3 + c) * 2 + 1];
+                Br[c] = Br[c] + (ar * er - ai * ei);
+                Bi[c] = Bi[c] + (ar * ei + ai * er);
+            }
+            ++q;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { out[kx * 6 + 2 * c] = Br[c]; out[kx * 6 + 2 * c + 1] = Bi[c]; }
+    }
+}
+
+template <class R>
+cudaError_t launch_btab(const double* modes, const R* trigy, const R* trigz, int ny, int nz, R* btab, cudaStream_t s) {
+    int rows = ny * nz;
+    btab_kernel<R><<<(rows + 255) / 256, 256, 0, s>>>(modes, trigy, trigz, ny, nz, btab);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// initial conditions
+// ------------------------------------------------------------------------------------------
+template <class R>
+__global__ void ic_ot_kernel(const Planes<R> u, int nx, int ny, int nz, double gamma) {
+    size_t n = (size_t)nx * ny * nz;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(c % nx), j = (int)((c / nx) % ny);
+        const double pi = 3.14159265358979323846, twopi = 2.0 * pi;
+        double x = (i + 0.5) / nx, y = (j + 0.5) / ny;
+        double rho = 25.0 / (36.0 * pi), pr = 5.0 / (12.0 * pi);
+        double vx = -sin(twopi * y), vy = sin(twopi * x);
+        double sb = 1.0 / sqrt(4.0 * pi);
+        double bx = -sb * sin(twopi * y), by = sb * sin(2.0 * twopi * x);
+        double ekin = 0.5 * rho * (vx * vx + vy * vy), emag = 0.5 * (bx * bx + by * by);
+        double v9[9] = {rho, rho * vx, rho * vy, 0.0, pr / (gamma - 1.0) + ekin + emag, bx, by, 0.0, 0.0};
+#pragma unroll
+        for (int v = 0; v < 9; ++v) u.p[v][c] = (R)v9[v];
+    }
+}
+
+template <class R>
+cudaError_t launch_ic_ot(const Planes<R>& u, int nx, int ny, int nz, double gamma, cudaStream_t s) {
+    size_t n = (size_t)nx * ny * nz;
+    int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    ic_ot_kernel<R><<<nb, 256, 0, s>>>(u, nx, ny, nz, gamma);
+    return cudaGetLastError();
+}
+
+template <class R> struct V9 { double v[9]; };
+
+template <class R>
+__global__ void ic_uniform_kernel(const Planes<R> u, size_t n, const V9<R> val) {
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int v = 0; v < 9; ++v) u.p[v][c] = (R)val.v[v];
+    }
+}
+
+template <class R>
+cudaError_t launch_ic_uniform(const Planes<R>& u, size_t n, const double v9[9], cudaStream_t s) {
+    V9<R> val;
+    for (int v = 0; v < 9; ++v) val.v[v] = v9[v];
+    int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    ic_uniform_kernel<R><<<nb, 256, 0, s>>>(u, n, val);
+    return cudaGetLastError();
+}
+
+template <class R>
+__global__ void ct_ic_ot_kernel(const Planes8<R> qv, int nx, int ny, int nz, double gamma, int phase) {
+    R* const* q = qv.p;
+    size_t n = (size_t)nx * ny * nz;
+    const double pi = 3.14159265358979323846, twopi = 2.0 * pi;
+    const double sb = 1.0 / sqrt(4.0 * pi);
+    const double dx = 1.0 / nx, dy = 1.0 / ny;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+        auto Az = [&](double x, double y) {
+            return sb * (cos(twopi * y) / twopi + cos(2.0 * twopi * x) / (2.0 * twopi));
+        };
+        if (phase == 0) {
+            double xl = i * dx, yl = j * dy;
+            q[5][c] = (R)((Az(xl, yl + dy) - Az(xl, yl)) / dy);
+            q[6][c] = (R)(-(Az(xl + dx, yl) - Az(xl, yl)) / dx);
+            q[7][c] = (R)0;
+        } else {
+            double x = (i + 0.5) * dx, y = (j + 0.5) * dy;
+            double rho = 25.0 / (36.0 * pi), pr = 5.0 / (12.0 * pi);
+            double vx = -sin(twopi * y), vy = sin(twopi * x);
+            size_t cxp = (size_t)wrapi(i + 1, nx) + (size_t)nx * (j + (size_t)ny * k);
+            size_t cyp = (size_t)i + (size_t)nx * (wrapi(j + 1, ny) + (size_t)ny * k);
+            double bx = 0.5 * ((double)q[5][c] + (double)q[5][cxp]);
+            double by = 0.5 * ((double)q[6][c] + (double)q[6][cyp]);
+            double ekin = 0.5 * rho * (vx * vx + vy * vy), emag = 0.5 * (bx * bx + by * by);
+            q[0][c] = (R)rho; q[1][c] = (R)(rho * vx); q[2][c] = (R)(rho * vy); q[3][c] = (R)0;
+            q[4][c] = (R)(pr / (gamma - 1.0) + ekin + emag);
+        }
+    }
+}
+
+template <class R>
+cudaError_t launch_ct_ic_ot(const Planes8<R>& q, int nx, int ny, int nz, double gamma, cudaStream_t s) {
+    size_t n = (size_t)nx * ny * nz;
+    int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    ct_ic_ot_kernel<R><<<nb, 256, 0, s>>>(q, nx, ny, nz, gamma, 0);
+    ct_ic_ot_kernel<R><<<nb, 256, 0, s>>>(q, nx, ny, nz, gamma, 1);
+    return cudaGetLastError();
+}
+
+// Seeded synthetic turbulent state: uniform (rho0, p0, B0) with v = vscale*a(x), dB = bscale*a(x),
+// rho = rho0*exp(0.2*a_y(x)), where a(x) is one stationary draw of the solenoidal 61-mode field
+// with unit rms (the forcing's own mode sum).  Stand-in for a pre-evolved turbulent checkpoint.
+template <class R>
+__global__ void ic_turb_kernel(const Planes<R> u, int nx, int ny, int nz, const R* btab, const R* trigx, double rho0,
+                               double p0, double b0x, double b0y, double b0z, double vscale, double bscale,
+                               double gamma) {
+    size_t n = (size_t)nx * ny * nz;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+        R ax, ay, az;
+        force_accel(btab + ((size_t)k * ny + j) * 24, trigx, nx, i, R(1), ax, ay, az);
+        double rho = rho0 * exp(0.2 * (double)ay);
+        double vx = vscale * (double)ax, vy = vscale * (double)ay, vz = vscale * (double)az;
+        double bx = b0x + bscale * (double)ax, by = b0y + bscale * (double)ay, bz = b0z + bscale * (double)az;
+        double e = p0 / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy + vz * vz) + 0.5 * (bx * bx + by * by + bz * bz);
+        double v9[9] = {rho, rho * vx, rho * vy, rho * vz, e, bx, by, bz, 0.0};
+#pragma unroll
+        for (int v = 0; v < 9; ++v) u.p[v][c] = (R)v9[v];
+    }
+}
+
+template <class R>
+cudaError_t launch_ic_turb(const Planes<R>& u, int nx, int ny, int nz, const R* btab, const R* trigx, double rho0,
+                           double p0, const double b0[3], double vscale, double bscale, double gamma, cudaStream_t s) {
+    size_t n = (size_t)nx * ny * nz;
+    int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    ic_turb_kernel<R><<<nb, 256, 0, s>>>(u, nx, ny, nz, btab, trigx, rho0, p0, b0[0], b0[1], b0[2], vscale, bscale,
+                                        gamma);
+    return cudaGetLastError();
+}
+
+#define GMT_INST(R)                                                                                              \
+    template cudaError_t launch_cfl<R>(const CPlanes<R>&, size_t, const Consts<R>&, unsigned long long*,         \
+                                       cudaStream_t);                                                            \
+    template cudaError_t launch_ct_cfl<R>(const CPlanes8<R>&, int, int, int, const Consts<R>&, unsigned long long*, \
+                                          cudaStream_t);                                                         \
+    template cudaError_t launch_diag<R>(const CPlanes<R>&, int, int, int, double, double, double*, int, double*, \
+                                        cudaStream_t);                                                           \
+    template cudaError_t launch_ct_divb<R>(const CPlanes8<R>&, int, int, int, double, unsigned long long*,          \
+                                           cudaStream_t);                                                        \
+    template cudaError_t launch_btab<R>(const double*, const R*, const R*, int, int, R*, cudaStream_t);          \
+    template cudaError_t launch_ic_ot<R>(const Planes<R>&, int, int, int, double, cudaStream_t);                 \
+    template cudaError_t launch_ic_uniform<R>(const Planes<R>&, size_t, const double*, cudaStream_t);            \
+    template cudaError_t launch_ic_turb<R>(const Planes<R>&, int, int, int, const R*, const R*, double, double,       \
+                                           const double*, double, double, double, cudaStream_t);                 \
+    template cudaError_t launch_ct_ic_ot<R>(const Planes8<R>&, int, int, int, double, cudaStream_t);
+GMT_INST(float)
+GMT_INST(double)
+
+}  // namespace gmt

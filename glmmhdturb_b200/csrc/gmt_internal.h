@@ -1,0 +1,71 @@
+// gmt_internal.h -- launchers shared between the kernel translation units and the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gmt_common.cuh"
+
+namespace gmt {
+
+constexpr int NMODES = 61;
+
+// unsplit GLM step (gmt_unsplit_f32.cu / gmt_unsplit_f64.cu)
+cudaError_t launch_unsplit(const UnsplitArgs<float>& A, int recon, int riem, cudaStream_t s);
+cudaError_t launch_unsplit(const UnsplitArgs<double>& A, int recon, int riem, cudaStream_t s);
+int unsplit_max_threads(int dtype_bytes);
+size_t unsplit_smem(int dtype_bytes, int ox, int oy);
+int unsplit_regs(int dtype_bytes, int recon, int riem);
+
+// transverse-free 1-D Hancock march (gmt_march1d.cu)
+template <class R> struct MarchArgs {
+    CPlanes<R> u;
+    Planes<R> o;
+    int nx, ny, nz, ox, oy, lz;
+    R dtdx, ch, glm_fac;
+    Consts<R> K;
+    int ppm;
+};
+cudaError_t launch_march1d(const MarchArgs<float>& A, cudaStream_t s);
+cudaError_t launch_march1d(const MarchArgs<double>& A, cudaStream_t s);
+int march1d_regs(int dtype_bytes);
+
+// constrained transport (gmt_ct.cu): q = [rho, mx, my, mz, E, bxf, byf, bzf]
+template <class R> struct CTArgs {
+    CPlanes8<R> q;
+    Planes8<R> o;
+    int nx, ny, nz, ox, oy, lz;
+    R dt, dtdx, ramp;
+    Consts<R> K;
+    int recon, riem, emf, halfslope, do_turb;
+    const R* btab;
+    const R* trigx;
+    R* scratch;            // 27 planes: lower-face fluxes F[3][8] and edge EMFs E[3]
+};
+cudaError_t launch_ct(const CTArgs<float>& A, cudaStream_t s);
+cudaError_t launch_ct(const CTArgs<double>& A, cudaStream_t s);
+int ct_regs_of(int dtype_bytes);
+size_t ct_smem_of(int dtype_bytes, int ox, int oy);
+
+// auxiliary kernels (gmt_aux.cu)
+template <class R> cudaError_t launch_cfl(const CPlanes<R>& u, size_t n, const Consts<R>& K,
+                                          unsigned long long* out, cudaStream_t s);
+template <class R> cudaError_t launch_ct_cfl(const CPlanes8<R>& q, int nx, int ny, int nz, const Consts<R>& K,
+                                             unsigned long long* out, cudaStream_t s);
+// diagnostics partials -> double out[10] = {mass, ke2, etot, psi2, divb2, divbmax, rhomin, nonfinite, -, -}
+template <class R> cudaError_t launch_diag(const CPlanes<R>& u, int nx, int ny, int nz, double dx, double smallr,
+                                           double* partials, int nblocks, double* out, cudaStream_t s);
+template <class R> cudaError_t launch_ct_divb(const CPlanes8<R>& q, int nx, int ny, int nz, double dx,
+                                              unsigned long long* out, cudaStream_t s);
+cudaError_t launch_ou_update(double* modes, uint32_t seed, uint32_t counter, double alpha, double beta,
+                             double sigma0, cudaStream_t s);
+template <class R> cudaError_t launch_btab(const double* modes, const R* trigy, const R* trigz, int ny, int nz,
+                                           R* btab, cudaStream_t s);
+template <class R> cudaError_t launch_ic_ot(const Planes<R>& u, int nx, int ny, int nz, double gamma, cudaStream_t s);
+template <class R> cudaError_t launch_ic_uniform(const Planes<R>& u, size_t n, const double v9[9], cudaStream_t s);
+template <class R> cudaError_t launch_ct_ic_ot(const Planes8<R>& q, int nx, int ny, int nz, double gamma, cudaStream_t s);
+template <class R> cudaError_t launch_ic_turb(const Planes<R>& u, int nx, int ny, int nz, const R* btab,
+                                             const R* trigx, double rho0, double p0, const double b0[3],
+                                             double vscale, double bscale, double gamma, cudaStream_t s);
+cudaError_t upload_mode_table();   // the 61 wavevectors into constant memory
+
+}  // namespace gmt

@@ -1,0 +1,285 @@
+// gmt_unsplit.cuh -- fused unsplit GLM-MHD step: PLM(MC|minmod)/PPM + MUSCL-Hancock +
+// HLLD|HLL|LLF + Dedner GLM + void floor + psi damping + mode-sum forcing kick (+ next-step CFL).
+//
+// Layout.  A block owns an OX x OY column tile of the periodic box over a chunk of LZ planes and
+// marches z.  Shared memory holds
+//   PR[3][9][(OX+4)(OY+4)]  primitive ring (planes k-1, k, k+1; 2-cell in-plane halo),
+//   ST[4][9][(OX+2)(OY+2)]  in-plane interface states +x,-x,+y,-y of the reconstruction region,
+//                           overwritten in place by the face fluxes,
+//   SG[9][(OX+4)(OY+4)]     conserved staging plane k+2, filled by cp.async while plane k computes.
+// Each owned thread keeps its column's z-face work in registers: the +z state of plane k-1,
+// F_z at the lower face and the x/y flux divergence of plane k-1, so every face is solved once
+// and every cell is read from HBM once and written once.
+//
+// Reference semantics: integrator_tiled!/integrator_plm!/integrator_plm_ppm!
+// (glmmhd_turb.jl:608-743, 782-864, 931-1014) -- one reconstruction per cell, one Riemann solve
+// per face, revert unphysical interface states (iflo, :618), update with floor, psi *= glm_fac,
+// forcing kick; the streaming order follows integrator_stream! (:1842-1946).
+#pragma once
+#include "gmt_common.cuh"
+
+namespace gmt {
+
+template <class R> struct Rec {
+    Q9<R> m0, mh, s[3];
+    bool up;
+};
+
+template <class R, int RECON>
+__device__ __forceinline__ void recon_prims(const R* __restrict__ PR, int PN, int PW, int c, int s0, int sm, int sp,
+                                            const Consts<R>& K, R dtdx, Rec<R>& r) {
+    const R* P0 = PR + (size_t)s0 * 9 * PN;
+    const R* Pm = PR + (size_t)sm * 9 * PN;
+    const R* Pp = PR + (size_t)sp * 9 * PN;
+    Q9<R> L, Rr;
+    constexpr bool MM = RECON == RECON_MINMOD;
+    bool up = true;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) r.m0.v[v] = P0[v * PN + c];
+#pragma unroll
+    for (int v = 0; v < 9; ++v) { L.v[v] = P0[v * PN + c - 1]; Rr.v[v] = P0[v * PN + c + 1]; }
+    r.s[0] = half_slope<MM>(L, r.m0, Rr);
+    if (RECON == RECON_PPM) up = up && !spj(L.v[4], r.m0.v[4], Rr.v[4]);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) { L.v[v] = P0[v * PN + c - PW]; Rr.v[v] = P0[v * PN + c + PW]; }
+    r.s[1] = half_slope<MM>(L, r.m0, Rr);
+    if (RECON == RECON_PPM) up = up && !spj(L.v[4], r.m0.v[4], Rr.v[4]);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) { L.v[v] = Pm[v * PN + c]; Rr.v[v] = Pp[v * PN + c]; }
+    r.s[2] = half_slope<MM>(L, r.m0, Rr);
+    if (RECON == RECON_PPM) up = up && !spj(L.v[4], r.m0.v[4], Rr.v[4]);
+    r.up = up;
+    r.mh = cons2prim(hancock(r.m0, r.s[0], r.s[1], r.s[2], dtdx, K.gamma), K.gamma, K.smallr, K.pfl);
+    if (r.mh.v[0] <= K.smallr || r.mh.v[4] <= K.pfl) r.mh = r.m0;
+}
+
+// interface state of the reconstructed cell on the SIGN side of axis D
+template <class R, int RECON, int D, int SIGN>
+__device__ __forceinline__ Q9<R> face_state(const Rec<R>& r, const R* __restrict__ PR, int PN, int PW, int c,
+                                            int s0, int sm, int sp, const Consts<R>& K, int iflo) {
+    Q9<R> f;
+    if (RECON == RECON_PPM && r.up) {
+        const R* PL;
+        const R* PRr;
+        int cl, cr;
+        if (D == 0) { PL = PRr = PR + (size_t)s0 * 9 * PN; cl = c - 1; cr = c + 1; }
+        else if (D == 1) { PL = PRr = PR + (size_t)s0 * 9 * PN; cl = c - PW; cr = c + PW; }
+        else { PL = PR + (size_t)sm * 9 * PN; PRr = PR + (size_t)sp * 9 * PN; cl = c; cr = c; }
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            R lo, hi;
+            ppm_edges(PL[v * PN + cl], r.m0.v[v], PRr[v * PN + cr], lo, hi);
+            f.v[v] = r.mh.v[v] + (SIGN > 0 ? hi : lo) - r.m0.v[v];
+        }
+    } else {
+        f = padd(r.mh, r.s[D], SIGN > 0 ? R(1) : R(-1));
+    }
+    if (iflo && (f.v[0] < K.smallr || f.v[4] < K.pfl)) f = r.m0;
+    return f;
+}
+
+template <class R> __device__ __forceinline__ void st_put(R* __restrict__ S, int RN, int idx, const Q9<R>& q) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) S[v * RN + idx] = q.v[v];
+}
+template <class R> __device__ __forceinline__ Q9<R> st_get(const R* __restrict__ S, int RN, int idx) {
+    Q9<R> q;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) q.v[v] = S[v * RN + idx];
+    return q;
+}
+
+__device__ __forceinline__ int mod3(int k) {
+    int m = k % 3;
+    return m < 0 ? m + 3 : m;
+}
+
+template <class R>
+__device__ __forceinline__ void stage_plane(R* __restrict__ SG, const CPlanes<R>& u, int PN, int PW, int x0, int y0,
+                                            int kp, int nx, int ny, int nz, int tid, int nt) {
+    const int gz = wrapi(kp, nz);
+    for (int c = tid; c < PN; c += nt) {
+        int lx = c % PW, ly = c / PW;
+        int gx = wrapi(x0 - 2 + lx, nx), gy = wrapi(y0 - 2 + ly, ny);
+        size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * gz);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) cp_async_r(SG + v * PN + c, u.p[v] + g);
+    }
+    cp_async_commit();
+}
+
+template <class R>
+__device__ __forceinline__ void unstage_plane(R* __restrict__ PRs, const R* __restrict__ SG, int PN, const Consts<R>& K,
+                                              int tid, int nt) {
+    for (int c = tid; c < PN; c += nt) {
+        Q9<R> q;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) q.v[v] = SG[v * PN + c];
+        q = cons2prim(q, K.gamma, K.smallr, K.pfl);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) PRs[v * PN + c] = q.v[v];
+    }
+}
+
+template <class R> __host__ __device__ inline size_t unsplit_smem_bytes(int ox, int oy) {
+    size_t PN = (size_t)(ox + 4) * (oy + 4), RN = (size_t)(ox + 2) * (oy + 2);
+    return (27 * PN + 36 * RN + 9 * PN) * sizeof(R) + 64 * sizeof(double);
+}
+
+template <class R, int RECON, int RIEM, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int OX = A.ox, OY = A.oy;
+    const int PW = OX + 4, PN = (OX + 4) * (OY + 4);
+    const int RW = OX + 2, RN = (OX + 2) * (OY + 2);
+    R* PR = reinterpret_cast<R*>(smem_raw);
+    R* ST = PR + 27 * PN;
+    R* SG = ST + 36 * RN;
+    double* red = reinterpret_cast<double*>(SG + 9 * PN);
+
+    const int tid = threadIdx.x, NT = OX * OY;
+    const int tx = tid % OX, ty = tid / OX;
+    const int x0 = blockIdx.x * OX, y0 = blockIdx.y * OY;
+    const int z0 = blockIdx.z * A.lz, z1 = min(z0 + A.lz, A.nz);
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const Consts<R> K = A.K;
+    const R dtdx = A.dtdx, ch = A.ch;
+    const bool turb = A.do_turb && A.btab != nullptr;
+    const int nhelp = 2 * (OX + OY);
+
+    // prologue: prims of planes z0-2, z0-1; conserved plane z0 left in flight
+    stage_plane(SG, A.u, PN, PW, x0, y0, z0 - 2, nx, ny, nz, tid, NT);
+    cp_async_wait_all();
+    __syncthreads();
+    unstage_plane(PR + mod3(z0 - 2) * 9 * PN, SG, PN, K, tid, NT);
+    __syncthreads();
+    stage_plane(SG, A.u, PN, PW, x0, y0, z0 - 1, nx, ny, nz, tid, NT);
+    cp_async_wait_all();
+    __syncthreads();
+    unstage_plane(PR + mod3(z0 - 1) * 9 * PN, SG, PN, K, tid, NT);
+    __syncthreads();
+    stage_plane(SG, A.u, PN, PW, x0, y0, z0, nx, ny, nz, tid, NT);
+
+    Q9<R> pPz, Fzlo, XY;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) { pPz.v[v] = R(0); Fzlo.v[v] = R(0); XY.v[v] = R(0); }
+    double cmax = 0.0, smax = 0.0;
+    const int gx = x0 + tx, gy = y0 + ty;
+    const int cown = (tx + 2) + PW * (ty + 2);     // ring-local index of the owned cell
+    const int rown = (tx + 1) + RW * (ty + 1);     // recon-local index of the owned cell
+
+    for (int kr = z0 - 1; kr <= z1; ++kr) {
+        const bool first = kr == z0 - 1, last = kr == z1;
+        const int s0 = mod3(kr), sm = mod3(kr - 1), sp = mod3(kr + 1);
+        // [L] plane kr+1: staging -> primitive ring
+        cp_async_wait_all();
+        __syncthreads();
+        unstage_plane(PR + sp * 9 * PN, SG, PN, K, tid, NT);
+        __syncthreads();
+        if (kr + 2 <= z1 + 1) stage_plane(SG, A.u, PN, PW, x0, y0, kr + 2, nx, ny, nz, tid, NT);
+
+        // [R] reconstruction of plane kr
+        {
+            Rec<R> r;
+            recon_prims<R, RECON>(PR, PN, PW, cown, s0, sm, sp, K, dtdx, r);
+            if (!first && !last) {
+                st_put(ST + 0 * 9 * RN, RN, rown, face_state<R, RECON, 0, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+                st_put(ST + 1 * 9 * RN, RN, rown, face_state<R, RECON, 0, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+                st_put(ST + 2 * 9 * RN, RN, rown, face_state<R, RECON, 1, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+                st_put(ST + 3 * 9 * RN, RN, rown, face_state<R, RECON, 1, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+            }
+            Q9<R> Pz = face_state<R, RECON, 2, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+            if (!first) {
+                Q9<R> Mz = face_state<R, RECON, 2, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+                Q9<R> Fzhi = riemann_glm<2, RIEM>(pPz, Mz, K, ch, A.use_llf != 0);
+                if (kr - 1 >= z0) {
+                    // finalize plane kr-1
+                    const int kf = kr - 1;
+                    const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * kf);
+                    Q9<R> q;
+#pragma unroll
+                    for (int v = 0; v < 9; ++v) q.v[v] = A.u.p[v][g] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
+                    R ax = R(0), ay = R(0), az = R(0);
+                    if (turb) force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, A.ramp, ax, ay, az);
+                    finish_update(q, K, A.glm_fac, turb, ax, ay, az, A.dt);
+#pragma unroll
+                    for (int v = 0; v < 9; ++v) A.o.p[v][g] = q.v[v];
+                    if (A.cfl_out) {
+                        R ct, sg;
+                        cfl_speeds(q, K, ct, sg);
+                        cmax = fmax(cmax, (double)ct);
+                        smax = fmax(smax, (double)sg);
+                    }
+                }
+                Fzlo = Fzhi;
+            }
+            pPz = Pz;
+        }
+        if (!first && !last) {
+            // halo reconstructions: only the one interface state each halo cell contributes
+            for (int h = tid; h < nhelp; h += NT) {
+                int rc, cc, which;
+                if (h < OY) { rc = 0 + RW * (h + 1); cc = 1 + PW * (h + 2); which = 0; }
+                else if (h < 2 * OY) { int f = h - OY; rc = (OX + 1) + RW * (f + 1); cc = (OX + 2) + PW * (f + 2); which = 1; }
+                else if (h < 2 * OY + OX) { int f = h - 2 * OY; rc = (f + 1); cc = (f + 2) + PW * 1; which = 2; }
+                else { int f = h - 2 * OY - OX; rc = (f + 1) + RW * (OY + 1); cc = (f + 2) + PW * (OY + 2); which = 3; }
+                Rec<R> r;
+                recon_prims<R, RECON>(PR, PN, PW, cc, s0, sm, sp, K, dtdx, r);
+                Q9<R> f;
+                if (which == 0) f = face_state<R, RECON, 0, +1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
+                else if (which == 1) f = face_state<R, RECON, 0, -1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
+                else if (which == 2) f = face_state<R, RECON, 1, +1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
+                else f = face_state<R, RECON, 1, -1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
+                st_put(ST + which * 9 * RN, RN, rc, f);
+            }
+        }
+        __syncthreads();
+        if (!first && !last) {
+            // [F] in-plane Riemann solves, flux written over the right state
+            {
+                const int ix = (tx + 2) + RW * (ty + 1);
+                Q9<R> F = riemann_glm<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, rown), st_get(ST + 1 * 9 * RN, RN, ix), K, ch,
+                                               A.use_llf != 0);
+                st_put(ST + 1 * 9 * RN, RN, ix, F);
+                const int iy = (tx + 1) + RW * (ty + 2);
+                F = riemann_glm<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, rown), st_get(ST + 3 * 9 * RN, RN, iy), K, ch,
+                                         A.use_llf != 0);
+                st_put(ST + 3 * 9 * RN, RN, iy, F);
+            }
+            for (int h = NT - 1 - tid; h < OX + OY; h += NT) {
+                // boundary faces on the low x and low y side, taken by the last threads
+                int f = h;
+                if (f < OY) {
+                    const int il = 0 + RW * (f + 1), ir = 1 + RW * (f + 1);
+                    Q9<R> F = riemann_glm<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, il), st_get(ST + 1 * 9 * RN, RN, ir), K,
+                                                   ch, A.use_llf != 0);
+                    st_put(ST + 1 * 9 * RN, RN, ir, F);
+                } else {
+                    const int c = f - OY;
+                    const int il = (c + 1), ir = (c + 1) + RW;
+                    Q9<R> F = riemann_glm<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, il), st_get(ST + 3 * 9 * RN, RN, ir), K,
+                                                   ch, A.use_llf != 0);
+                    st_put(ST + 3 * 9 * RN, RN, ir, F);
+                }
+            }
+            __syncthreads();
+            // [X] x/y flux divergence of the owned cell
+            {
+                const int ixh = (tx + 2) + RW * (ty + 1), iyh = (tx + 1) + RW * (ty + 2);
+#pragma unroll
+                for (int v = 0; v < 9; ++v) {
+                    const R* Sx = ST + (1 * 9 + v) * RN;
+                    const R* Sy = ST + (3 * 9 + v) * RN;
+                    XY.v[v] = (Sx[rown] - Sx[ixh]) + (Sy[rown] - Sy[iyh]);
+                }
+            }
+        }
+    }
+    if (A.cfl_out) {
+        block_max_atomic(cmax, A.cfl_out, red);
+        __syncthreads();
+        block_max_atomic(smax, A.cfl_out + 1, red);
+    }
+}
+
+}  // namespace gmt

@@ -1,0 +1,168 @@
+/* glmmhd_b200.h -- C ABI of libglmmhd_b200.so, the B200 (sm_100a) GLM-MHD / CT-MHD time step.
+ *
+ * Two layers:
+ *
+ *  1. The legacy bridge symbols, with the exact signatures the reference's Julia bridge binds
+ *     (march_bridge/MarchBridge.jl:34-81 via dlsym + ccall, march_bridge/cu/spike_mhd.cu:321-340,
+ *     march_bridge/cu/spike_ctm.cu:299-328).  `march_*` run the transverse-free 1-D Hancock + HLL
+ *     + Dedner march scheme; `ct_run` runs the constrained-transport march.  As in the reference,
+ *     they return elapsed ms and report no errors; the extended API below does.
+ *
+ *  2. The extended API (`gmt_*`): a context per configuration, explicit streams, FP32 and FP64,
+ *     runtime grid size, every scheme of the reference's Julia step API (glmmhd_turb.jl step_plm!
+ *     :878, step_tiled! :746, step_multi! :1981, compute_dt :1973; ct_mhd.jl CTMHD.step! :174),
+ *     status codes, and the deterministic mode-sum forcing.
+ *
+ * State layout everywhere: SoA planes of nx*ny*nz reals, x fastest,
+ * index = i + nx*(j + ny*k) -- the memory image of the reference's (N,N,N,9) Float32 array
+ * (glmmhd_turb.jl:57,63-64).  GLM: 9 planes [rho, rho vx, rho vy, rho vz, E, Bx, By, Bz, psi].
+ * CT: 8 planes [rho, rho vx, rho vy, rho vz, E, bxf, byf, bzf], bxf[i,j,k] = Bx on the lower-x
+ * face (ct_mhd.jl:10-11).  All data pointers are device pointers owned by the caller; `stream`
+ * is a cudaStream_t (NULL = legacy default stream).
+ */
+#ifndef GLMMHD_B200_H
+#define GLMMHD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GMT_ABI_VERSION 1
+
+/* status codes (0 = success) */
+enum {
+    GMT_OK = 0,
+    GMT_ERR_ARG = 1,         /* invalid argument / unsupported size */
+    GMT_ERR_CUDA = 2,        /* a CUDA call failed; see gmt_last_error() */
+    GMT_ERR_UNSUPPORTED = 3, /* configuration not built */
+    GMT_ERR_STATE = 4,       /* non-finite or non-positive state detected */
+    GMT_ERR_NOMEM = 5
+};
+enum { GMT_F32 = 0, GMT_F64 = 1 };
+enum { GMT_SCHEME_UNSPLIT = 0, GMT_SCHEME_MARCH1D = 1, GMT_SCHEME_CT = 2 };
+enum { GMT_RECON_MC = 0, GMT_RECON_MINMOD = 1, GMT_RECON_PPM = 2 };
+enum { GMT_RIEMANN_HLLD = 0, GMT_RIEMANN_HLL = 1, GMT_RIEMANN_LLF = 2, GMT_RIEMANN_LLF_BOUND = 3 };
+enum { GMT_EMF_AVERAGE = 0, GMT_EMF_CONTACT = 1 };
+
+/* Configuration.  Physical defaults follow `Params` (glmmhd_turb.jl:28-52); call
+ * gmt_params_init() and override fields. */
+typedef struct gmt_params {
+    int32_t abi_version;      /* GMT_ABI_VERSION */
+    int32_t nx, ny, nz;
+    int32_t dtype;            /* GMT_F32 | GMT_F64 */
+    int32_t scheme;           /* GMT_SCHEME_* */
+    int32_t recon;            /* GMT_RECON_* */
+    int32_t riemann;          /* GMT_RIEMANN_* */
+    int32_t iflo;             /* 1: revert unphysical interface states (glmmhd_turb.jl:618) */
+    int32_t emf;              /* CT edge EMF: GMT_EMF_* */
+    int32_t ct_halfslope;     /* CT: 1 = ct_mhd.jl's extra factor 1/2 on the slope (:49-50) */
+    int32_t tile_x, tile_y, tile_z; /* 0 = automatic */
+    int32_t pad0;
+    double boxlen, gamma, courant, smallr, smallc;
+    double smallp;            /* march / CT pressure floor (spike_mhd.cu:52) */
+    double glm_ch_scale, glm_cp_coef;
+    double llf_dmin, llf_pmin;
+    double turb_min_rho;
+    double turb_amp;          /* stationary rms acceleration of the forcing field */
+    double turb_T;            /* OU autocorrelation time */
+    int32_t turb_ndt;         /* OU updates per turb_T */
+    uint32_t turb_seed;
+} gmt_params;
+
+/* One step. */
+typedef struct gmt_step_args {
+    double dt;
+    double t;                 /* simulation time (forcing ramp min(t/turb_T, 1)) */
+    double ch;                /* GLM cleaning speed */
+    double glm_fac;           /* psi *= glm_fac after the update */
+    int32_t do_turb;          /* apply the forcing kick */
+    int32_t want_cfl;         /* fuse the next step's CFL reduction into this step */
+} gmt_step_args;
+
+typedef struct gmt_diag {
+    double mass, ke2, vrms, divbmax, rhomin, etot, divb_l2, psi_l2;
+    int32_t finite, nonfinite_cells;
+} gmt_diag;
+
+typedef struct gmt_ctx gmt_ctx;
+
+/* --- library / context ------------------------------------------------------------------ */
+const char* gmt_version(void);
+/* last error message of the calling thread ("" if none) */
+const char* gmt_last_error(void);
+/* fill reference defaults for an n^3 box (glmmhd_turb.jl:28-52) */
+int gmt_params_init(gmt_params* p, int n);
+/* allocate a context on the current device: scratch for reductions, forcing tables, tiles */
+int gmt_create(const gmt_params* p, gmt_ctx** out);
+int gmt_destroy(gmt_ctx* ctx);
+/* kernel resource report: registers, dynamic shared bytes and tile of the step kernel */
+int gmt_kernel_info(gmt_ctx* ctx, int32_t* regs, int64_t* smem_bytes, int32_t tile[3]);
+
+/* --- GLM step (unsplit: step_plm!/step_tiled!/step_multi!; march1d: march_run_dev) ------- */
+/* uold/unew: base pointers of 9 contiguous planes (plane stride nx*ny*nz) */
+int gmt_step(gmt_ctx* ctx, const void* uold, void* unew, const gmt_step_args* a, void* stream);
+/* same with one pointer per plane (the bridge's float*[9] layout) */
+int gmt_step_planes(gmt_ctx* ctx, const void* const* uold, void* const* unew, const gmt_step_args* a,
+                    void* stream);
+
+/* --- CFL (compute_dt, glmmhd_turb.jl:1963-1978) ------------------------------------------ */
+/* reduce max_cells sum_d(|v_d|+c_f) and max_cells max_d(|v_d|+c_f) into the context (async) */
+int gmt_cfl_async(gmt_ctx* ctx, const void* u, void* stream);
+/* synchronise `stream` and read the last CFL maxima (from gmt_cfl_async or a want_cfl step) */
+int gmt_cfl_result(gmt_ctx* ctx, double out[2], void* stream);
+/* dt = courant*dx/max ctot (synchronous, as compute_dt) */
+int gmt_compute_dt(gmt_ctx* ctx, const void* u, double* dt, void* stream);
+
+/* --- diagnostics (glmmhd_turb.jl:1996-2018), FP64, deterministic ------------------------- */
+int gmt_diagnostics(gmt_ctx* ctx, const void* u, gmt_diag* out, void* stream);
+
+/* --- forcing: 61 +/- integer modes, 1 <= |k|^2 <= 9, solenoidal OU, Philox4x32-10 -------- */
+int gmt_forcing_reset(gmt_ctx* ctx, void* stream);
+/* one OU update (interval turb_T/turb_ndt) + refresh of the per-row mode table */
+int gmt_forcing_advance(gmt_ctx* ctx, void* stream);
+/* host copies of the complex mode amplitudes, layout [61][3][2] doubles */
+int gmt_forcing_set_modes(gmt_ctx* ctx, const double* modes, void* stream);
+int gmt_forcing_get_modes(gmt_ctx* ctx, double* modes, void* stream);
+int gmt_forcing_counter(gmt_ctx* ctx, uint32_t* counter);
+
+/* --- initial conditions on the device ---------------------------------------------------- */
+int gmt_ic_orszag_tang(gmt_ctx* ctx, void* u, void* stream);            /* glmmhd_turb.jl:2021 */
+int gmt_ic_uniform(gmt_ctx* ctx, void* u, double rho0, double p0, double bx0, double by0, double bz0,
+                   void* stream);                                          /* glmmhd_turb.jl:2164 */
+/* seeded synthetic turbulent state (stand-in for a pre-evolved checkpoint): the uniform state plus
+ * v = mach*c_s*a(x), dB = db*a(x), rho = rho0*exp(0.2 a_y(x)), a = one unit-rms draw of the 61-mode
+ * solenoidal field with Philox seed `seed` */
+int gmt_ic_turbulent(gmt_ctx* ctx, void* u, double rho0, double p0, double bx0, double by0, double bz0,
+                     double mach, double db, uint32_t seed, void* stream);
+
+/* --- constrained transport (CTMHD.step!, ct_mhd.jl:174; ct_run, spike_ctm.cu:305) --------- */
+/* q: base pointer of 8 planes [rho, mx, my, mz, E, bxf, byf, bzf] */
+int gmt_ct_step(gmt_ctx* ctx, const void* qold, void* qnew, const gmt_step_args* a, void* stream);
+int gmt_ct_cfl_async(gmt_ctx* ctx, const void* q, void* stream);
+/* max |div B| from the face field (ct_mhd.jl:190-194) */
+int gmt_ct_divb_max(gmt_ctx* ctx, const void* q, double* out, void* stream);
+int gmt_ct_ic_orszag_tang(gmt_ctx* ctx, void* q, void* stream);
+
+/* --- legacy bridge ABI (march_bridge/MarchBridge.jl, spike_mhd.cu:321-340) --------------- */
+/* The grid size of the legacy entry points is fixed when the library is built (GMT_LEGACY_NX,
+ * as build_mhd.sh's -DNX) and may be changed at run time with march_set_nx. */
+int march_nv(void);                              /* 9 (+ passive species: 0) */
+int march_nx(void);
+int march_nsp(void);
+void march_set_dtdx(float v);
+void march_set_glm(float ch, float glmfac);
+void march_set_gamma(float g);
+double march_run_dev(float* const* qv, float* const* ov, int nsteps);
+void march_set_nx(int n);                        /* extension: runtime grid size */
+/* CT march (spike_ctm.cu:299-328): qv/ov = 5 conserved + 3 face-B planes, cc = 3 scratch planes */
+double ct_run(float* const* qv, float* const* ov, float* const* cc, int nsteps);
+int ct_regs(void);
+int ct_shmem(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GLMMHD_B200_H */

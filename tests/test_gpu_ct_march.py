@@ -1,0 +1,125 @@
+"""GPU parity of the CT step, the 1-D Hancock march scheme and the legacy bridge ABI."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from tests.golden import make_golden as G
+from tests.gpu_util import max_rel_err, to_dev
+
+pytestmark = pytest.mark.gpu
+
+MARCH = [c for c in G.CASES if c[1] == "march1d"]
+CT = [c for c in G.CASES if c[1] == "ct"]
+
+
+def _solver(case, dtype, n=G.N, **kw):
+    from glmmhdturb_b200 import Solver
+    name, scheme, recon, riem, iflo, emf, half, turb = case
+    return Solver(n, dtype=dtype, scheme=scheme, recon=recon, riemann=riem, iflo=iflo, emf=emf or "average",
+                  ct_halfslope=half, gamma=G.GAMMA, smallp=1e-6, turb_T=1.0, **kw)
+
+
+@pytest.mark.parametrize("case", MARCH + CT, ids=[c[0] for c in MARCH + CT])
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_golden(golden, case, dtype):
+    s = _solver(case, dtype)
+    tdt = torch.float64 if dtype == "f64" else torch.float32
+    src = golden["ct_in"] if case[1] == "ct" else golden["glm_in"]
+    u = to_dev(src, tdt)
+    out = torch.empty_like(u)
+    if case[7]:
+        s.set_modes(golden["modes"])
+    s.step(u, out, G.DT, t=G.RAMP, ch=G.CH, glm_fac=G.FAC, do_turb=case[7])
+    err, errs = max_rel_err(out.cpu().numpy(), golden[case[0]])
+    print(f"{case[0]} {dtype}: max rel err {err:.3e}")
+    assert err <= (1e-12 if dtype == "f64" else 3e-5), errs
+
+
+@pytest.mark.parametrize("emf,riem", [("average", "hll"), ("contact", "hlld")])
+def test_ct_noncubic_vs_oracle_and_divb(oracle, emf, riem):
+    from glmmhdturb_b200 import Solver
+    n = (24, 16, 12)
+    cfg = oracle.Config(n=n, gamma=5 / 3, riemann=riem, emf=emf)
+    q0 = oracle.ct_ic_ot(cfg)
+    rng = np.random.default_rng(3)
+    q0[1:4] += 0.05 * rng.standard_normal(q0[1:4].shape)
+    s = Solver(n, dtype="f64", scheme="ct", riemann=riem, emf=emf, gamma=5 / 3)
+    q = to_dev(q0)
+    w = torch.empty_like(q)
+    ref = q0
+    for _ in range(5):
+        cmax, _ = oracle.ct_cfl(cfg, ref)
+        dt = 0.3 * cfg.dx / cmax
+        ref = oracle.ct_step(cfg, ref, dt)
+        s.step(q, w, dt)
+        q, w = w, q
+    err, errs = max_rel_err(q.cpu().numpy(), ref)
+    assert err <= 1e-12, errs
+    assert s.ct_divb_max(q) < 1e-11
+
+
+def test_ct_fp32_divb_roundoff():
+    from glmmhdturb_b200 import Solver
+    s = Solver(32, dtype="f32", scheme="ct", riemann="hlld", emf="contact", gamma=5 / 3)
+    q = s.alloc()
+    s.ic_orszag_tang(q)
+    w = torch.empty_like(q)
+    d0 = s.ct_divb_max(q)
+    for _ in range(20):
+        dt = 0.3 * s.dx / s.cfl(q)[0]
+        s.step(q, w, dt)
+        q, w = w, q
+    assert s.ct_divb_max(q) < 1e-4 and d0 < 1e-4   # FP32 round-off floor (BENCHMARKS.md:60-62)
+
+
+def _legacy_planes(src, nvar):
+    q = [torch.from_numpy(np.ascontiguousarray(src[v])).float().cuda() for v in range(nvar)]
+    o = [torch.zeros_like(x) for x in q]
+    return q, o
+
+
+@pytest.mark.parametrize("nsteps", [1, 2, 3])
+def test_march_run_dev_legacy_abi(golden, nsteps):
+    """march_run_dev over a host array of device plane pointers (MarchBridge.jl:64-81)."""
+    from glmmhdturb_b200 import Solver, march_bridge as MB
+    m = MB.open_lib()
+    m.h.march_set_nx(G.N[0])
+    m = MB.open_lib()
+    assert m.NV == 9 and m.N == G.N[0] and m.has_glm
+    MB.set_gamma(m, G.GAMMA)
+    MB.set_dtdx(m, G.DT / (1.0 / G.N[0]))
+    MB.set_glm(m, G.CH, G.FAC)
+    q, o = _legacy_planes(golden["glm_in"], 9)
+    ms = MB.run(m, q, o, nsteps)
+    assert ms >= 0.0
+    got = torch.stack(q).cpu().numpy()
+    s = Solver(G.N, dtype="f32", scheme="march1d", riemann="hll", gamma=G.GAMMA, smallp=1e-6)
+    u = to_dev(golden["glm_in"], torch.float32)
+    w = torch.empty_like(u)
+    dt = float(np.float32(G.DT / (1.0 / G.N[0]))) * (1.0 / G.N[0])
+    for _ in range(nsteps):
+        s.step(u, w, dt, ch=float(np.float32(G.CH)), glm_fac=float(np.float32(G.FAC)))
+        u, w = w, u
+    assert np.array_equal(got, u.cpu().numpy())
+    if nsteps == 1:
+        err, _ = max_rel_err(got, golden["march_plm"])
+        assert err < 3e-5
+
+
+def test_ct_run_legacy_abi(golden):
+    from glmmhdturb_b200 import _lib
+    L = _lib.lib()
+    L.march_set_nx(G.N[0])
+    L.march_set_gamma(C.c_float(G.GAMMA))
+    L.march_set_dtdx(C.c_float(G.DT * G.N[0]))
+    q, o = _legacy_planes(golden["ct_in"], 8)
+    cc = [torch.zeros_like(q[0]) for _ in range(3)]
+    arr = lambda xs: C.cast((C.c_void_p * len(xs))(*[x.data_ptr() for x in xs]), C.c_void_p)  # noqa: E731
+    ms = L.ct_run(arr(q), arr(o), arr(cc), 1)
+    assert ms >= 0.0
+    got = torch.stack(q).cpu().numpy()
+    err, errs = max_rel_err(got, golden["ct_plm_hll_avg"])
+    assert err < 3e-5, errs
+    assert L.ct_regs() > 0

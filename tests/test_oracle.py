@@ -1,0 +1,130 @@
+"""CPU tests of the oracle: pins against the reference's published numbers, known-answer
+vectors of the RNG, forcing definition, and the committed golden fixtures."""
+import numpy as np
+import pytest
+
+from tests.golden import make_golden as G
+
+
+def test_orszag_tang_64_hlld_pin(oracle):
+    # validate_tiled_ot (glmmhd_turb.jl:2278): N=64, gamma=5/3, courant 0.7, t_end 0.2, HLLD.
+    # Published: vrms 0.7887, div.B 2.9 (REPORT.md:24-26; BENCHMARKS.md:179), fp32 on an A6000.
+    cfg = oracle.Config(n=(64, 64, 1), gamma=5 / 3, recon="mc", riemann="hlld", iflo=True)
+    _, d = oracle.run_ot(cfg, t_end=0.2, courant=0.7)
+    assert d["finite"]
+    assert abs(d["vrms"] - 0.7887) < 5e-4
+    assert abs(d["divbmax"] - 2.9) < 0.1
+    assert abs(d["rhomin"] - 0.0835) < 1e-3
+
+
+def test_orszag_tang_120_ppm_hll_pin(oracle):
+    # BENCHMARKS.md:178: N=120 MHD PPM(+HLL): vrms 0.7910, div.B 1.16, rhomin 0.0835
+    cfg = oracle.Config(n=(120, 120, 1), gamma=5 / 3, recon="ppm", riemann="hll", iflo=True)
+    _, d = oracle.run_ot(cfg, t_end=0.2, courant=0.7)
+    assert abs(d["vrms"] - 0.7910) < 5e-4
+    assert abs(d["divbmax"] - 1.16) < 0.05
+    assert abs(d["rhomin"] - 0.0835) < 1e-3
+
+
+def test_multikernel_equals_tiled_on_ot(oracle):
+    # BENCHMARKS.md:179: tiled (iflo) and multi-kernel paths are identical on OT (no revert fires)
+    a = oracle.Config(n=(32, 32, 1), gamma=5 / 3, iflo=True)
+    b = oracle.Config(n=(32, 32, 1), gamma=5 / 3, iflo=False)
+    ua, _ = oracle.run_ot(a, t_end=0.05)
+    ub, _ = oracle.run_ot(b, t_end=0.05)
+    assert np.array_equal(ua, ub)
+
+
+def test_philox_known_answers(oracle):
+    # Philox4x32-10 known-answer vectors (Salmon et al., SC'11 / Random123 kat_vectors)
+    assert [hex(x) for x in oracle.philox([0, 0, 0, 0], [0, 0])] == \
+        ["0x6627e8d5", "0xe169c58d", "0xbc57ac4c", "0x9b00dbd8"]
+    assert [hex(x) for x in oracle.philox([0xffffffff] * 4, [0xffffffff] * 2)] == \
+        ["0x408f276d", "0x41c83b0e", "0xa20bc7c6", "0x6d5451fd"]
+    assert [hex(x) for x in oracle.philox([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344],
+                                          [0xa4093822, 0x299f31d0])] == \
+        ["0xd16cfe09", "0x94fdcceb", "0x5001e420", "0x24126ea1"]
+
+
+def test_mode_table(oracle):
+    k = oracle.mode_k()
+    k2 = (k ** 2).sum(1)
+    assert k.shape == (61, 3) and k2.min() == 1 and k2.max() == 9
+    # half space, no +-k duplicates, sorted by kx
+    keys = {tuple(r) for r in k}
+    assert len(keys) == 61 and not any(tuple(-np.array(r)) in keys for r in k)
+    assert (np.diff(k[:, 0]) >= 0).all()
+    # all 122 integer vectors with 1 <= |k|^2 <= 9 are covered by +-k
+    allk = {(a, b, c) for a in range(-3, 4) for b in range(-3, 4) for c in range(-3, 4) if 1 <= a*a+b*b+c*c <= 9}
+    assert len(allk) == 122 and keys | {tuple(-np.array(r)) for r in k} == allk
+
+
+def test_forcing_is_solenoidal_and_normalised(oracle):
+    f = oracle.OUForcing(amp=2.0, T=0.5, ndt=100, seed=3)
+    k = oracle.mode_k().astype(float)
+    acc = []
+    for i in range(2000):
+        f.advance()
+        if i > 200 and i % 10 == 0:
+            m = f.modes
+            # k . ahat = 0 (real and imaginary parts)
+            assert np.abs(np.einsum("qc,qcr->qr", k, m)).max() < 1e-12
+            acc.append(2.0 * (m ** 2).sum())     # <|a|^2> = sum_H 2|ahat|^2
+    rms = np.sqrt(np.mean(acc))
+    assert 0.8 * 2.0 < rms < 1.2 * 2.0
+
+
+def test_accel_matches_direct_mode_sum(oracle):
+    cfg = oracle.Config(n=(8, 6, 4))
+    f = oracle.OUForcing(amp=1.0, seed=1)
+    f.advance()
+    a = oracle.accel(cfg, f.modes, ramp=0.5)
+    k = oracle.mode_k()
+    nx, ny, nz = cfg.n
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    z = (np.arange(nz) + 0.5) / nz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    ref = np.zeros((3, nz, ny, nx))
+    for q in range(61):
+        th = 2 * np.pi * (k[q, 0] * X + k[q, 1] * Y + k[q, 2] * Z)
+        for c in range(3):
+            ref[c] += 2 * (f.modes[q, c, 0] * np.cos(th) - f.modes[q, c, 1] * np.sin(th))
+    np.testing.assert_allclose(a, 0.5 * ref, atol=1e-13)
+
+
+def test_fp32_oracle_tracks_fp64(oracle, golden):
+    cfg = G.cfg_of(G.CASES[0])
+    u = golden["glm_in"]
+    r64 = oracle.step_unsplit(cfg, u, G.DT, G.CH, G.FAC, G.RAMP, golden["modes"])
+    r32 = oracle.step_unsplit(cfg, u.astype(np.float32), G.DT, G.CH, G.FAC, G.RAMP, golden["modes"])
+    for v in range(9):
+        scale = max(np.abs(r64[v]).max(), 1e-30)
+        assert np.abs(r32[v] - r64[v]).max() / scale < 2e-5
+
+
+@pytest.mark.parametrize("case", G.CASES, ids=[c[0] for c in G.CASES])
+def test_oracle_reproduces_golden(oracle, golden, case):
+    fresh = G.compute() if not hasattr(test_oracle_reproduces_golden, "_c") else test_oracle_reproduces_golden._c
+    test_oracle_reproduces_golden._c = fresh
+    assert np.array_equal(fresh[case[0]], golden[case[0]])
+
+
+def test_ct_oracle_preserves_divb(oracle):
+    cfg = oracle.Config(n=(16, 16, 8), gamma=5 / 3, riemann="hlld", emf="contact")
+    q = oracle.ct_ic_ot(cfg)
+    rng = np.random.default_rng(1)
+    q[1:4] += 0.05 * rng.standard_normal(q[1:4].shape)
+    d0 = oracle.ct_divb_max(cfg, q)
+    for _ in range(10):
+        cmax, _ = oracle.ct_cfl(cfg, q)
+        q = oracle.ct_step(cfg, q, 0.3 * cfg.dx / cmax)
+    assert d0 < 1e-12 and oracle.ct_divb_max(cfg, q) < 1e-11
+
+
+def test_conservation_unsplit(oracle, golden):
+    cfg = G.cfg_of(G.CASES[1])
+    u = golden["glm_in"]
+    r = oracle.step_unsplit(cfg, u, G.DT, G.CH, 1.0)
+    for v in range(8):   # rho, momentum, E, B conserved by the flux form (psi has no source at fac=1)
+        assert abs(r[v].sum() - u[v].sum()) <= 1e-12 * max(np.abs(u[v]).sum(), 1.0)
