@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--riemann", default="hlld")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--tile", default="", help="force tile as X,Y,Z")
     return ap.parse_args()
 
 
@@ -236,10 +238,21 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(args.dtype, args.recon, args.riemann)
 
-    from glmmhdturb_b200 import Solver
+    from glmmhdturb_b200 import Solver, autotune
     n = args.n
+    tile, tuned = (0, 0, 0), None
+    if args.tile:
+        tile = tuple(int(v) for v in args.tile.split(","))
+    elif not args.no_tune:
+        c = autotune.cached(n, args.dtype, "unsplit", args.recon, args.riemann)
+        if c:
+            tile, tuned = tuple(c["tile"]), {"source": "cache", "ms": c["ms"]}
+        else:
+            tile, ms, res = autotune.tune(n, dtype=args.dtype, recon=args.recon, riemann=args.riemann)
+            tuned = {"source": "autotune", "ms": ms, "candidates": len(res),
+                     "top": [[list(t), round(m, 3)] for m, t in res[:6]]}
     s = Solver(n, dtype=args.dtype, recon=args.recon, riemann=args.riemann, gamma=GAMMA, courant=COURANT,
-               turb_amp=AMP, turb_T=0.5, turb_ndt=100, turb_seed=1)
+               turb_amp=AMP, turb_T=0.5, turb_ndt=100, turb_seed=1, tile=tile)
     stream = torch.cuda.current_stream()
     u = s.alloc()
     w = s.alloc()
@@ -356,7 +369,7 @@ def run_ours(args):
                "data": "synthetic",
                "config": workload_config(args, {"parallelism": f"replicas{world}" if world > 1 else "single",
                                                 "tile": list(info["tile"]), "regs": info["regs"],
-                                                "smem_bytes": info["smem"]}),
+                                                "smem_bytes": info["smem"], "autotune": tuned}),
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "peak_source": peak_src,
                             "traffic": (tb * zones if tb else None),

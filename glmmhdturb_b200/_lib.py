@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libglmmhd_b200.so")
 CSRC = os.path.join(HERE, "csrc")
 
 GMT_ABI_VERSION = 1
-GMT_OK, GMT_ERR_ARG, GMT_ERR_CUDA, GMT_ERR_UNSUPPORTED, GMT_ERR_STATE, GMT_ERR_NOMEM = range(6)
+GMT_OK, GMT_ERR_ARG, GMT_ERR_CUDA, GMT_ERR_UNSUPPORTED, GMT_ERR_STATE, GMT_ERR_NOMEM, GMT_ERR_TIMEOUT = range(7)
 F32, F64 = 0, 1
 SCHEME = {"unsplit": 0, "march1d": 1, "ct": 2}
 RECON = {"mc": 0, "plm": 0, "minmod": 1, "ppm": 2}

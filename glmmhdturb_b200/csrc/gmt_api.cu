@@ -75,6 +75,7 @@ struct gmt_ctx {
     void* trig[3] = {nullptr, nullptr, nullptr};
     void* ct_scratch = nullptr;
     unsigned long long* divb = nullptr;
+    int* err = nullptr;       // device flag set by kernels whose bounded waits gave up
     uint32_t counter = 0;
     double sigma0 = 0, alpha = 0, beta = 0;
 };
@@ -106,7 +107,8 @@ int choose_tile(gmt_ctx* c) {
     }
     if (!divides(p.nx, ox) || !divides(p.ny, oy))
         return fail(GMT_ERR_ARG, "tile " + std::to_string(ox) + "x" + std::to_string(oy) + " does not divide the grid");
-    if (ox * oy > 256) return fail(GMT_ERR_ARG, "tile_x*tile_y must be <= 256");
+    if (ox * oy > unsplit_max_threads(c->esize))
+        return fail(GMT_ERR_ARG, "tile_x*tile_y must be <= " + std::to_string(unsplit_max_threads(c->esize)));
     if (unsplit_smem(c->esize, ox, oy) > 227 * 1024) return fail(GMT_ERR_ARG, "tile needs more than 227 KB shared memory");
     int lz = p.tile_z;
     if (lz <= 0) {
@@ -148,6 +150,7 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.btab = a->do_turb ? static_cast<const R*>(c->btab) : nullptr;
         A.trigx = static_cast<const R*>(c->trig[0]);
         A.cfl_out = nullptr;
+        A.err = c->err;
         if (a->want_cfl) {
             GMT_CUDA(cudaMemsetAsync(c->cfl, 0, 2 * sizeof(unsigned long long), s));
             A.cfl_out = c->cfl;
@@ -306,6 +309,8 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     for (int a = 0; ok && a < 3; ++a) ok = alloc(&c->trig[a], (size_t)8 * dims[a] * c->esize);
     if (ok && p->scheme == GMT_SCHEME_CT) ok = alloc(&c->ct_scratch, (size_t)27 * c->n * c->esize);
     if (ok) ok = alloc((void**)&c->divb, sizeof(unsigned long long));
+    if (ok) ok = alloc((void**)&c->err, sizeof(int));
+    if (ok && cudaMemset(c->err, 0, sizeof(int)) != cudaSuccess) ok = false;
     if (!ok) { gmt_destroy(c); return GMT_ERR_NOMEM; }
     for (int a = 0; a < 3; ++a) {
         std::vector<double> t = trig_table(dims[a]);
@@ -343,6 +348,7 @@ int gmt_destroy(gmt_ctx* c) {
     for (auto& t : c->trig) cudaFree(t);
     cudaFree(c->ct_scratch);
     cudaFree(c->divb);
+    cudaFree(c->err);
     delete c;
     return GMT_OK;
 }
@@ -352,7 +358,8 @@ int gmt_kernel_info(gmt_ctx* c, int32_t* regs, int64_t* smem, int32_t tile[3]) {
     int r = -1;
     int64_t sm = 0;
     if (c->p.scheme == GMT_SCHEME_UNSPLIT) {
-        r = unsplit_regs(c->esize, c->p.recon, c->p.riemann == GMT_RIEMANN_LLF ? GMT_RIEMANN_HLLD : c->p.riemann);
+        r = unsplit_regs(c->esize, c->p.recon, c->p.riemann == GMT_RIEMANN_LLF ? GMT_RIEMANN_HLLD : c->p.riemann,
+                         c->ox * c->oy);
         sm = (int64_t)unsplit_smem(c->esize, c->ox, c->oy);
     } else if (c->p.scheme == GMT_SCHEME_MARCH1D) {
         r = march1d_regs(c->esize);
@@ -401,8 +408,14 @@ int gmt_cfl_async(gmt_ctx* c, const void* u, void* stream) {
 int gmt_cfl_result(gmt_ctx* c, double out[2], void* stream) {
     if (!c || !out) return fail(GMT_ERR_ARG, "gmt_cfl_result: null argument");
     unsigned long long h[2];
+    int herr = 0;
     GMT_CUDA(cudaMemcpyAsync(h, c->cfl, sizeof(h), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    GMT_CUDA(cudaMemcpyAsync(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     GMT_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    if (herr) {
+        cudaMemsetAsync(c->err, 0, sizeof(int), (cudaStream_t)stream);
+        return fail(GMT_ERR_TIMEOUT, "a step kernel abandoned a bounded wait; its output is invalid");
+    }
     std::memcpy(&out[0], &h[0], 8);
     std::memcpy(&out[1], &h[1], 8);
     if (!std::isfinite(out[0]) || !(out[0] > 0.0)) return fail(GMT_ERR_STATE, "CFL maximum is not positive and finite");
@@ -695,12 +708,12 @@ int ct_shmem(void) { return (int)ct_smem_of(4, 0, 0); }
 }  // extern "C"
 
 namespace gmt {
-int unsplit_regs_f32(int recon, int riem);
-int unsplit_regs_f64(int recon, int riem);
-int unsplit_regs(int esize, int recon, int riem) {
-    return esize == 8 ? unsplit_regs_f64(recon, riem) : unsplit_regs_f32(recon, riem);
+int unsplit_regs_f32(int recon, int riem, int nthreads);
+int unsplit_regs_f64(int recon, int riem, int nthreads);
+int unsplit_regs(int esize, int recon, int riem, int nthreads) {
+    return esize == 8 ? unsplit_regs_f64(recon, riem, nthreads) : unsplit_regs_f32(recon, riem, nthreads);
 }
-int unsplit_max_threads(int) { return 256; }
+int unsplit_max_threads(int esize) { return esize == 8 ? 256 : 512; }
 size_t unsplit_smem(int esize, int ox, int oy) {
     return esize == 8 ? unsplit_smem_bytes<double>(ox, oy) : unsplit_smem_bytes<float>(ox, oy);
 }

@@ -30,6 +30,7 @@ template <class R> struct UnsplitArgs {
     const R* btab;         // forcing row table [nz][ny][4 kx][3 comp][2] (re, im) or null
     const R* trigx;        // [4 m][2 cos|sin][nx]
     unsigned long long* cfl_out;  // [2] bits of non-negative doubles (max ctot, max signal) or null
+    int* err;              // set to 1 when a bounded wait gives up (never expected)
 };
 
 // cp.async 4-byte global -> shared copy (L1-allocating), plus group commit / wait.
@@ -43,6 +44,34 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// mbarrier completion of cp.async groups: every thread arrives once per phase after issuing its
+// copies; the phase completes when all of them have landed in shared memory.
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(s), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive_cp_async(uint64_t* bar) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(s) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(bar);
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(s), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: gives up after ~2^20 polls, records the failure and returns false
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+    for (int it = 0; it < (1 << 20); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicExch(err, 1);
+    return false;
+}
 
 template <class R> __device__ __forceinline__ void cp_async_r(R* smem, const R* gmem);
 template <> __device__ __forceinline__ void cp_async_r(float* s, const float* g) { cp_async4(s, g); }

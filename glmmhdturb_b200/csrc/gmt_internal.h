@@ -14,7 +14,7 @@ cudaError_t launch_unsplit(const UnsplitArgs<float>& A, int recon, int riem, cud
 cudaError_t launch_unsplit(const UnsplitArgs<double>& A, int recon, int riem, cudaStream_t s);
 int unsplit_max_threads(int dtype_bytes);
 size_t unsplit_smem(int dtype_bytes, int ox, int oy);
-int unsplit_regs(int dtype_bytes, int recon, int riem);
+int unsplit_regs(int dtype_bytes, int recon, int riem, int nthreads);
 
 // transverse-free 1-D Hancock march (gmt_march1d.cu)
 template <class R> struct MarchArgs {

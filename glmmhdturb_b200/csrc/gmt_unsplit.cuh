@@ -7,9 +7,10 @@
 //   ST[4][9][(OX+2)(OY+2)]  in-plane interface states +x,-x,+y,-y of the reconstruction region,
 //                           overwritten in place by the face fluxes,
 //   SG[9][(OX+4)(OY+4)]     conserved staging plane k+2, filled by cp.async while plane k computes.
-// Each owned thread keeps its column's z-face work in registers: the +z state of plane k-1,
-// F_z at the lower face and the x/y flux divergence of plane k-1, so every face is solved once
-// and every cell is read from HBM once and written once.
+// Each owned thread keeps its column's z-face work in registers (the +z state of plane k-1 and
+// F_z at its lower face) plus its own x/y face fluxes, so every face is solved once, every cell is
+// read from HBM once and written once, and a plane costs two block barriers.  The next conserved
+// plane streams in by cp.async and completes on an mbarrier (bounded wait, error flag).
 //
 // Reference semantics: integrator_tiled!/integrator_plm!/integrator_plm_ppm!
 // (glmmhd_turb.jl:608-743, 782-864, 931-1014) -- one reconstruction per cell, one Riemann solve
@@ -123,7 +124,7 @@ __device__ __forceinline__ void unstage_plane(R* __restrict__ PRs, const R* __re
 
 template <class R> __host__ __device__ inline size_t unsplit_smem_bytes(int ox, int oy) {
     size_t PN = (size_t)(ox + 4) * (oy + 4), RN = (size_t)(ox + 2) * (oy + 2);
-    return (27 * PN + 36 * RN + 9 * PN) * sizeof(R) + 64 * sizeof(double);
+    return (27 * PN + 36 * RN + 9 * PN) * sizeof(R) + 40 * sizeof(double);
 }
 
 template <class R, int RECON, int RIEM, int MAXT, int MINB>
@@ -147,39 +148,49 @@ __global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R
     const bool turb = A.do_turb && A.btab != nullptr;
     const int nhelp = 2 * (OX + OY);
 
-    // prologue: prims of planes z0-2, z0-1; conserved plane z0 left in flight
-    stage_plane(SG, A.u, PN, PW, x0, y0, z0 - 2, nx, ny, nz, tid, NT);
-    cp_async_wait_all();
-    __syncthreads();
-    unstage_plane(PR + mod3(z0 - 2) * 9 * PN, SG, PN, K, tid, NT);
-    __syncthreads();
-    stage_plane(SG, A.u, PN, PW, x0, y0, z0 - 1, nx, ny, nz, tid, NT);
-    cp_async_wait_all();
-    __syncthreads();
-    unstage_plane(PR + mod3(z0 - 1) * 9 * PN, SG, PN, K, tid, NT);
-    __syncthreads();
-    stage_plane(SG, A.u, PN, PW, x0, y0, z0, nx, ny, nz, tid, NT);
+    // prologue: primitives of planes z0-2, z0-1, z0
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
+    for (int j = 0; j < 3; ++j) {
+        stage_plane(SG, A.u, PN, PW, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
+        cp_async_wait_all();
+        __syncthreads();
+        unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, SG, PN, K, tid, NT);
+        if (j == 2 && tid == 0) mbar_init(mbar, NT);
+        __syncthreads();
+    }
 
-    Q9<R> pPz, Fzlo, XY;
+    // registers carried along the column: +z state of the previous plane, F_z at its lower face,
+    // and this thread's own x/y face fluxes of the previous plane
+    Q9<R> pPz, Fzlo, Fxh, Fyh;
 #pragma unroll
-    for (int v = 0; v < 9; ++v) { pPz.v[v] = R(0); Fzlo.v[v] = R(0); XY.v[v] = R(0); }
+    for (int v = 0; v < 9; ++v) { pPz.v[v] = R(0); Fzlo.v[v] = R(0); Fxh.v[v] = R(0); Fyh.v[v] = R(0); }
     double cmax = 0.0, smax = 0.0;
     const int gx = x0 + tx, gy = y0 + ty;
     const int cown = (tx + 2) + PW * (ty + 2);     // ring-local index of the owned cell
     const int rown = (tx + 1) + RW * (ty + 1);     // recon-local index of the owned cell
+    const int ixh = (tx + 2) + RW * (ty + 1);      // slot of the +x neighbour
+    const int iyh = (tx + 1) + RW * (ty + 2);      // slot of the +y neighbour
+    unsigned phase = 0;
 
+    // Two barriers per plane:
+    //  [R] issue the load of plane kr+2; x/y divergence of plane kr-1 (own fluxes in registers,
+    //      lower-face fluxes from the own slot); reconstruct plane kr; F_z at kr-1/2; write out kr-1
+    //  [F] x/y Riemann solves of plane kr; convert plane kr+2 into the primitive ring
     for (int kr = z0 - 1; kr <= z1; ++kr) {
         const bool first = kr == z0 - 1, last = kr == z1;
+        const bool load = kr + 2 <= z1 + 1;
         const int s0 = mod3(kr), sm = mod3(kr - 1), sp = mod3(kr + 1);
-        // [L] plane kr+1: staging -> primitive ring
-        cp_async_wait_all();
-        __syncthreads();
-        unstage_plane(PR + sp * 9 * PN, SG, PN, K, tid, NT);
-        __syncthreads();
-        if (kr + 2 <= z1 + 1) stage_plane(SG, A.u, PN, PW, x0, y0, kr + 2, nx, ny, nz, tid, NT);
-
-        // [R] reconstruction of plane kr
+        if (load) {
+            stage_plane(SG, A.u, PN, PW, x0, y0, kr + 2, nx, ny, nz, tid, NT);
+            mbar_arrive_cp_async(mbar);
+        }
         {
+            Q9<R> XY;
+            if (kr - 1 >= z0) {
+#pragma unroll
+                for (int v = 0; v < 9; ++v)
+                    XY.v[v] = (ST[(1 * 9 + v) * RN + rown] - Fxh.v[v]) + (ST[(3 * 9 + v) * RN + rown] - Fyh.v[v]);
+            }
             Rec<R> r;
             recon_prims<R, RECON>(PR, PN, PW, cown, s0, sm, sp, K, dtdx, r);
             if (!first && !last) {
@@ -193,7 +204,6 @@ __global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R
                 Q9<R> Mz = face_state<R, RECON, 2, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
                 Q9<R> Fzhi = riemann_glm<2, RIEM>(pPz, Mz, K, ch, A.use_llf != 0);
                 if (kr - 1 >= z0) {
-                    // finalize plane kr-1
                     const int kf = kr - 1;
                     const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * kf);
                     Q9<R> q;
@@ -235,45 +245,36 @@ __global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R
         }
         __syncthreads();
         if (!first && !last) {
-            // [F] in-plane Riemann solves, flux written over the right state
-            {
-                const int ix = (tx + 2) + RW * (ty + 1);
-                Q9<R> F = riemann_glm<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, rown), st_get(ST + 1 * 9 * RN, RN, ix), K, ch,
-                                               A.use_llf != 0);
-                st_put(ST + 1 * 9 * RN, RN, ix, F);
-                const int iy = (tx + 1) + RW * (ty + 2);
-                F = riemann_glm<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, rown), st_get(ST + 3 * 9 * RN, RN, iy), K, ch,
-                                         A.use_llf != 0);
-                st_put(ST + 3 * 9 * RN, RN, iy, F);
-            }
+            // own faces at x+1/2 and y+1/2: flux kept in registers and written over the right state,
+            // where the neighbour reads it as its lower-face flux
+            Fxh = riemann_glm<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, rown), st_get(ST + 1 * 9 * RN, RN, ixh), K, ch,
+                                       A.use_llf != 0);
+            st_put(ST + 1 * 9 * RN, RN, ixh, Fxh);
+            Fyh = riemann_glm<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, rown), st_get(ST + 3 * 9 * RN, RN, iyh), K, ch,
+                                       A.use_llf != 0);
+            st_put(ST + 3 * 9 * RN, RN, iyh, Fyh);
             for (int h = NT - 1 - tid; h < OX + OY; h += NT) {
-                // boundary faces on the low x and low y side, taken by the last threads
-                int f = h;
-                if (f < OY) {
-                    const int il = 0 + RW * (f + 1), ir = 1 + RW * (f + 1);
+                // boundary faces on the low x and low y side of the tile, taken by the last threads
+                if (h < OY) {
+                    const int il = 0 + RW * (h + 1), ir = 1 + RW * (h + 1);
                     Q9<R> F = riemann_glm<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, il), st_get(ST + 1 * 9 * RN, RN, ir), K,
                                                    ch, A.use_llf != 0);
                     st_put(ST + 1 * 9 * RN, RN, ir, F);
                 } else {
-                    const int c = f - OY;
+                    const int c = h - OY;
                     const int il = (c + 1), ir = (c + 1) + RW;
                     Q9<R> F = riemann_glm<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, il), st_get(ST + 3 * 9 * RN, RN, ir), K,
                                                    ch, A.use_llf != 0);
                     st_put(ST + 3 * 9 * RN, RN, ir, F);
                 }
             }
-            __syncthreads();
-            // [X] x/y flux divergence of the owned cell
-            {
-                const int ixh = (tx + 2) + RW * (ty + 1), iyh = (tx + 1) + RW * (ty + 2);
-#pragma unroll
-                for (int v = 0; v < 9; ++v) {
-                    const R* Sx = ST + (1 * 9 + v) * RN;
-                    const R* Sy = ST + (3 * 9 + v) * RN;
-                    XY.v[v] = (Sx[rown] - Sx[ixh]) + (Sy[rown] - Sy[iyh]);
-                }
-            }
         }
+        if (load) {
+            mbar_wait(mbar, phase, A.err);
+            phase ^= 1u;
+            unstage_plane(PR + mod3(kr + 2) * 9 * PN, SG, PN, K, tid, NT);
+        }
+        __syncthreads();
     }
     if (A.cfl_out) {
         block_max_atomic(cmax, A.cfl_out, red);

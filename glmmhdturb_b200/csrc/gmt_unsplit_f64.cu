@@ -1,10 +1,11 @@
-// FP64 unsplit step kernels: 256 threads, 1 resident block per SM.  Built with --fmad=false so
-// each expression rounds exactly as the IEEE evaluation of the oracle.
+// FP64 unsplit step kernels: up to 256 threads, 1 resident block per SM.  Built with --fmad=false
+// so each expression rounds exactly as the IEEE evaluation of the oracle.
 #include "gmt_unsplit_inst.cuh"
 
 namespace gmt {
 cudaError_t launch_unsplit(const UnsplitArgs<double>& A, int recon, int riem, cudaStream_t s) {
-    return unsplit_dispatch<double, 256, 1>(A, recon, riem, s);
+    if (A.ox * A.oy > 256) return cudaErrorInvalidConfiguration;
+    return unsplit_dispatch_t<double, 256, 1>(A, recon, riem, s);
 }
-int unsplit_regs_f64(int recon, int riem) { return unsplit_regs_of<double, 256, 1>(recon, riem); }
+int unsplit_regs_f64(int recon, int riem, int) { return unsplit_regs_of_t<double, 256, 1>(recon, riem); }
 }  // namespace gmt

@@ -26,7 +26,7 @@ static cudaError_t unsplit_go(const UnsplitArgs<R>& A, cudaStream_t s) {
 }
 
 template <class R, int MAXT, int MINB>
-static cudaError_t unsplit_dispatch(const UnsplitArgs<R>& A, int recon, int riem, cudaStream_t s) {
+static cudaError_t unsplit_dispatch_t(const UnsplitArgs<R>& A, int recon, int riem, cudaStream_t s) {
 #define GMT_CASE(RC, RM) \
     if (recon == RC && riem == RM) return unsplit_go<R, RC, RM, MAXT, MINB>(A, s);
     GMT_CASE(RECON_MC, RIEM_HLLD) GMT_CASE(RECON_MC, RIEM_HLL) GMT_CASE(RECON_MC, RIEM_LLF_BOUND)
@@ -36,7 +36,7 @@ static cudaError_t unsplit_dispatch(const UnsplitArgs<R>& A, int recon, int riem
     return cudaErrorInvalidValue;
 }
 
-template <class R, int MAXT, int MINB> static int unsplit_regs_of(int recon, int riem) {
+template <class R, int MAXT, int MINB> static int unsplit_regs_of_t(int recon, int riem) {
     cudaFuncAttributes fa{};
     cudaError_t e = cudaErrorInvalidValue;
 #define GMT_CASE(RC, RM) \

@@ -39,7 +39,8 @@ enum {
     GMT_ERR_CUDA = 2,        /* a CUDA call failed; see gmt_last_error() */
     GMT_ERR_UNSUPPORTED = 3, /* configuration not built */
     GMT_ERR_STATE = 4,       /* non-finite or non-positive state detected */
-    GMT_ERR_NOMEM = 5
+    GMT_ERR_NOMEM = 5,
+    GMT_ERR_TIMEOUT = 6      /* a bounded in-kernel wait gave up; results of that step are invalid */
 };
 enum { GMT_F32 = 0, GMT_F64 = 1 };
 enum { GMT_SCHEME_UNSPLIT = 0, GMT_SCHEME_MARCH1D = 1, GMT_SCHEME_CT = 2 };
@@ -111,7 +112,8 @@ int gmt_step_planes(gmt_ctx* ctx, const void* const* uold, void* const* unew, co
 /* --- CFL (compute_dt, glmmhd_turb.jl:1963-1978) ------------------------------------------ */
 /* reduce max_cells sum_d(|v_d|+c_f) and max_cells max_d(|v_d|+c_f) into the context (async) */
 int gmt_cfl_async(gmt_ctx* ctx, const void* u, void* stream);
-/* synchronise `stream` and read the last CFL maxima (from gmt_cfl_async or a want_cfl step) */
+/* synchronise `stream` and read the last CFL maxima (from gmt_cfl_async or a want_cfl step);
+ * also reports GMT_ERR_TIMEOUT if a step since the last check abandoned a bounded wait */
 int gmt_cfl_result(gmt_ctx* ctx, double out[2], void* stream);
 /* dt = courant*dx/max ctot (synchronous, as compute_dt) */
 int gmt_compute_dt(gmt_ctx* ctx, const void* u, double* dt, void* stream);
