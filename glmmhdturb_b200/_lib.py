@@ -21,11 +21,12 @@ RECON = {"mc": 0, "plm": 0, "minmod": 1, "ppm": 2}
 RIEMANN = {"hlld": 0, "hll": 1, "llf": 2, "llf_bound": 3}
 EMF = {"average": 0, "contact": 1}
 NMODES = 61
+NOALLOC_MAX_PLANES = 2048
 
 # every symbol declared in include/glmmhd_b200.h
 EXPORTS = (
     "gmt_version", "gmt_last_error", "gmt_params_init", "gmt_create", "gmt_destroy", "gmt_kernel_info",
-    "gmt_step", "gmt_step_planes", "gmt_cfl_async", "gmt_cfl_result", "gmt_compute_dt", "gmt_diagnostics",
+    "gmt_step", "gmt_step_planes", "gmt_cfl_async", "gmt_cfl_result", "gmt_compute_dt", "gmt_diagnostics", "gmt_diagnostics_noalloc",
     "gmt_forcing_reset", "gmt_forcing_advance", "gmt_forcing_set_modes", "gmt_forcing_get_modes",
     "gmt_forcing_counter", "gmt_ic_orszag_tang", "gmt_ic_uniform", "gmt_ic_turbulent", "gmt_ct_step", "gmt_ct_cfl_async",
     "gmt_ct_divb_max", "gmt_ct_ic_orszag_tang", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
@@ -89,6 +90,7 @@ def lib():
             "gmt_cfl_async": ([vp, vp, vp], C.c_int), "gmt_cfl_result": ([vp, C.POINTER(dbl), vp], C.c_int),
             "gmt_compute_dt": ([vp, vp, C.POINTER(dbl), vp], C.c_int),
             "gmt_diagnostics": ([vp, vp, C.POINTER(GmtDiag), vp], C.c_int),
+            "gmt_diagnostics_noalloc": ([vp, i32, i32, i32, i32, dbl, dbl, C.POINTER(GmtDiag), vp], C.c_int),
             "gmt_forcing_reset": ([vp, vp], C.c_int), "gmt_forcing_advance": ([vp, vp], C.c_int),
             "gmt_forcing_set_modes": ([vp, C.POINTER(dbl), vp], C.c_int),
             "gmt_forcing_get_modes": ([vp, C.POINTER(dbl), vp], C.c_int),

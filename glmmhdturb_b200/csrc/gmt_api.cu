@@ -708,6 +708,7 @@ int ct_shmem(void) { return (int)ct_smem_of(4, 0, 0); }
 }  // extern "C"
 
 namespace gmt {
+void set_last_error(const std::string& msg) { g_err = msg; }
 int unsplit_regs_f32(int recon, int riem, int nthreads);
 int unsplit_regs_f64(int recon, int riem, int nthreads);
 int unsplit_regs(int esize, int recon, int riem, int nthreads) {

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "gmt_common.cuh"
 
 namespace gmt {
@@ -67,5 +69,6 @@ template <class R> cudaError_t launch_ic_turb(const Planes<R>& u, int nx, int ny
                                              const R* trigx, double rho0, double p0, const double b0[3],
                                              double vscale, double bscale, double gamma, cudaStream_t s);
 cudaError_t upload_mode_table();   // the 61 wavevectors into constant memory
+void set_last_error(const std::string& msg);   // message returned by gmt_last_error() on this thread
 
 }  // namespace gmt

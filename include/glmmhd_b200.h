@@ -121,6 +121,19 @@ int gmt_compute_dt(gmt_ctx* ctx, const void* u, double* dt, void* stream);
 /* --- diagnostics (glmmhd_turb.jl:1996-2018), FP64, deterministic ------------------------- */
 int gmt_diagnostics(gmt_ctx* ctx, const void* u, gmt_diag* out, void* stream);
 
+/* --- diagnostics without allocation --------------------------------------------------------
+ * No counterpart in the reference.  Same quantities as gmt_diagnostics for a 9-plane GLM state,
+ * for callers that must not allocate device memory: a driver loop that cannot afford the device
+ * synchronisation of cudaMalloc/cudaFree, a host framework whose own pool owns the memory budget,
+ * or a hook holding only a state pointer and no context.  Allocates nothing: its scratch is a
+ * static device array in the library image (one row per z-plane), so nz is limited to
+ * GMT_NOALLOC_MAX_PLANES (GMT_ERR_ARG beyond it).  The first call on a device looks up that
+ * array's device address; make it before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller.  Synchronous on `stream`. */
+#define GMT_NOALLOC_MAX_PLANES 2048
+int gmt_diagnostics_noalloc(const void* u, int32_t nx, int32_t ny, int32_t nz, int32_t dtype, double boxlen,
+                            double smallr, gmt_diag* out, void* stream);
+
 /* --- forcing: 61 +/- integer modes, 1 <= |k|^2 <= 9, solenoidal OU, Philox4x32-10 -------- */
 int gmt_forcing_reset(gmt_ctx* ctx, void* stream);
 /* one OU update (interval turb_T/turb_ndt) + refresh of the per-row mode table */
