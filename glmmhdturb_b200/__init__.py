@@ -9,6 +9,6 @@ host-side mirror of the reference's step API:
     glmmhdturb_b200.Solver        a configured engine over device tensors
 """
 from ._lib import GmtError, build, lib, version  # noqa: F401
-from .solver import Solver  # noqa: F401
+from .solver import Ensemble, Solver  # noqa: F401
 
-__all__ = ["Solver", "GmtError", "build", "lib", "version"]
+__all__ = ["Solver", "Ensemble", "GmtError", "build", "lib", "version"]

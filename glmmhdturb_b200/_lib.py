@@ -22,6 +22,7 @@ RIEMANN = {"hlld": 0, "hll": 1, "llf": 2, "llf_bound": 3}
 EMF = {"average": 0, "contact": 1}
 NMODES = 61
 NOALLOC_MAX_PLANES = 2048
+RUN_CH_MAXSIGNAL, RUN_FORCING, RUN_GRAPH = 1, 2, 4
 
 # every symbol declared in include/glmmhd_b200.h
 EXPORTS = (
@@ -29,7 +30,8 @@ EXPORTS = (
     "gmt_step", "gmt_step_planes", "gmt_cfl_async", "gmt_cfl_result", "gmt_compute_dt", "gmt_diagnostics", "gmt_diagnostics_noalloc",
     "gmt_forcing_reset", "gmt_forcing_advance", "gmt_forcing_set_modes", "gmt_forcing_get_modes",
     "gmt_forcing_counter", "gmt_ic_orszag_tang", "gmt_ic_uniform", "gmt_ic_turbulent", "gmt_ct_step", "gmt_ct_cfl_async",
-    "gmt_ct_divb_max", "gmt_ct_ic_orszag_tang", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
+    "gmt_ct_divb_max", "gmt_ct_ic_orszag_tang", "gmt_ke_spectrum", "gmt_run", "gmt_ensemble_create", "gmt_ensemble_destroy",
+    "gmt_ensemble_run", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
     "march_set_glm", "march_set_gamma", "march_run_dev", "march_set_nx", "ct_run", "ct_regs", "ct_shmem",
 )
 
@@ -101,6 +103,12 @@ def lib():
             "gmt_ct_step": ([vp, vp, vp, A, vp], C.c_int), "gmt_ct_cfl_async": ([vp, vp, vp], C.c_int),
             "gmt_ct_divb_max": ([vp, vp, C.POINTER(dbl), vp], C.c_int),
             "gmt_ct_ic_orszag_tang": ([vp, vp, vp], C.c_int),
+            "gmt_ke_spectrum": ([vp, vp, i32, C.POINTER(dbl), vp], C.c_int),
+            "gmt_run": ([vp, vp, vp, i32, dbl, dbl, i32, vp, C.POINTER(dbl), C.POINTER(i32)], C.c_int),
+            "gmt_ensemble_create": ([P, i32, C.POINTER(i32), C.POINTER(dbl), C.POINTER(C.c_uint32), C.POINTER(vp)],
+                                    C.c_int),
+            "gmt_ensemble_destroy": ([vp], C.c_int),
+            "gmt_ensemble_run": ([vp, vp, vp, i32, dbl, i32, vp, C.POINTER(dbl)], C.c_int),
             "march_nv": ([], C.c_int), "march_nx": ([], C.c_int), "march_nsp": ([], C.c_int),
             "march_set_dtdx": ([C.c_float], None), "march_set_glm": ([C.c_float, C.c_float], None),
             "march_set_gamma": ([C.c_float], None), "march_set_nx": ([C.c_int], None),

@@ -1,4 +1,5 @@
 // gmt_api.cu -- C ABI of libglmmhd_b200.so (declared in include/glmmhd_b200.h).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -9,6 +10,7 @@
 #include "../../include/glmmhd_b200.h"
 #include "gmt_internal.h"
 #include "gmt_unsplit.cuh"
+#include "gmt_loop.cuh"
 
 using namespace gmt;
 
@@ -76,6 +78,16 @@ struct gmt_ctx {
     void* ct_scratch = nullptr;
     unsigned long long* divb = nullptr;
     int* err = nullptr;       // device flag set by kernels whose bounded waits gave up
+    LoopState* loop = nullptr;     // device-resident time loop record (gmt_run)
+    LoopConst* loopc = nullptr;
+    void* bt = nullptr;            // BoxTables<R> of this box
+    const int* mode_k_dev = nullptr;
+    cudaStream_t cap = nullptr;    // private stream for graph capture
+    struct Graph { const void* u; const void* w; int flags; cudaGraphExec_t exec; };
+    std::vector<Graph> graphs;
+    double next_time = 0.0;        // next forcing update time
+    void* spec = nullptr;          // spectrum scratch (grown on demand)
+    size_t spec_bytes = 0;
     uint32_t counter = 0;
     double sigma0 = 0, alpha = 0, beta = 0;
 };
@@ -151,6 +163,8 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.trigx = static_cast<const R*>(c->trig[0]);
         A.cfl_out = nullptr;
         A.err = c->err;
+        A.dx = (R)dx;
+        A.dparams = nullptr;
         if (a->want_cfl) {
             GMT_CUDA(cudaMemsetAsync(c->cfl, 0, 2 * sizeof(unsigned long long), s));
             A.cfl_out = c->cfl;
@@ -286,6 +300,10 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
         return fail(GMT_ERR_UNSUPPORTED, "gmt_create: CT supports MC and PPM reconstruction");
     std::call_once(g_mode_once, [] { g_mode_err = upload_mode_table(); });
     if (g_mode_err != cudaSuccess) return cuda_fail(g_mode_err, "mode table");
+    {
+        cudaError_t e = p->dtype == GMT_F64 ? unsplit_prepare_f64() : unsplit_prepare_f32();
+        if (e != cudaSuccess) return cuda_fail(e, "kernel attributes");
+    }
 
     gmt_ctx* c = new gmt_ctx();
     c->p = *p;
@@ -310,6 +328,8 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     if (ok && p->scheme == GMT_SCHEME_CT) ok = alloc(&c->ct_scratch, (size_t)27 * c->n * c->esize);
     if (ok) ok = alloc((void**)&c->divb, sizeof(unsigned long long));
     if (ok) ok = alloc((void**)&c->err, sizeof(int));
+    if (ok) ok = alloc((void**)&c->loop, sizeof(LoopState)) && alloc((void**)&c->loopc, sizeof(LoopConst)) &&
+                 alloc(&c->bt, sizeof(BoxTables<double>));
     if (ok && cudaMemset(c->err, 0, sizeof(int)) != cudaSuccess) ok = false;
     if (!ok) { gmt_destroy(c); return GMT_ERR_NOMEM; }
     for (int a = 0; a < 3; ++a) {
@@ -330,6 +350,20 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     c->sigma0 = forcing_sigma0(p->turb_amp, c->alpha, c->beta);
     rc = gmt_forcing_reset(c, nullptr);
     if (rc == GMT_OK) {
+        cudaError_t e = mode_table_device(&c->mode_k_dev);
+        if (e == cudaSuccess) {
+            if (c->esize == 8) {
+                BoxTables<double> T{c->modes, (const double*)c->trig[1], (const double*)c->trig[2], (double*)c->btab, p->ny, p->nz};
+                e = cudaMemcpy(c->bt, &T, sizeof(T), cudaMemcpyHostToDevice);
+            } else {
+                BoxTables<float> T{c->modes, (const float*)c->trig[1], (const float*)c->trig[2], (float*)c->btab, p->ny, p->nz};
+                e = cudaMemcpy(c->bt, &T, sizeof(T), cudaMemcpyHostToDevice);
+            }
+        }
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
+        if (e != cudaSuccess) rc = cuda_fail(e, "gmt_create");
+    }
+    if (rc == GMT_OK) {
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) rc = cuda_fail(e, "gmt_create");
     }
@@ -349,6 +383,12 @@ int gmt_destroy(gmt_ctx* c) {
     cudaFree(c->ct_scratch);
     cudaFree(c->divb);
     cudaFree(c->err);
+    for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
+    cudaFree(c->spec);
+    if (c->cap) cudaStreamDestroy(c->cap);
+    cudaFree(c->loop);
+    cudaFree(c->loopc);
+    cudaFree(c->bt);
     delete c;
     return GMT_OK;
 }
@@ -457,11 +497,32 @@ int gmt_diagnostics(gmt_ctx* c, const void* u, gmt_diag* out, void* stream) {
     return GMT_OK;
 }
 
+int gmt_ke_spectrum(gmt_ctx* c, const void* u, int32_t kmax, double* out, void* stream) {
+    if (!c || !u || !out) return fail(GMT_ERR_ARG, "gmt_ke_spectrum: null argument");
+    if (c->p.scheme == GMT_SCHEME_CT) return fail(GMT_ERR_ARG, "gmt_ke_spectrum: GLM state only");
+    if (kmax < 1 || 2 * kmax + 1 > std::min(c->p.ny, c->p.nz) || kmax + 1 > c->p.nx)
+        return fail(GMT_ERR_ARG, "gmt_ke_spectrum: need 1 <= kmax and 2*kmax+1 <= grid size");
+    size_t need = spectrum_scratch_bytes(c->p.nx, c->p.ny, c->p.nz, kmax);
+    if (need > c->spec_bytes) {
+        cudaFree(c->spec);
+        c->spec = nullptr;
+        c->spec_bytes = 0;
+        GMT_CUDA(cudaMalloc(&c->spec, need));
+        c->spec_bytes = need;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = c->esize == 8
+                        ? launch_spectrum<double>(cplanes<double>(u, c->n), c->p.nx, c->p.ny, c->p.nz, kmax, c->spec, out, s)
+                        : launch_spectrum<float>(cplanes<float>(u, c->n), c->p.nx, c->p.ny, c->p.nz, kmax, c->spec, out, s);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_ke_spectrum");
+}
+
 int gmt_forcing_reset(gmt_ctx* c, void* stream) {
     if (!c) return fail(GMT_ERR_ARG, "null context");
     cudaStream_t s = (cudaStream_t)stream;
     GMT_CUDA(cudaMemsetAsync(c->modes, 0, NMODES * 6 * sizeof(double), s));
     c->counter = 0;
+    c->next_time = 0.0;
     return refresh_btab_any(c, s);
 }
 
@@ -471,6 +532,7 @@ int gmt_forcing_advance(gmt_ctx* c, void* stream) {
     cudaError_t e = launch_ou_update(c->modes, c->p.turb_seed, c->counter, c->alpha, c->beta, c->sigma0, s);
     if (e != cudaSuccess) return cuda_fail(e, "OU update");
     c->counter++;
+    c->next_time += c->p.turb_T / (c->p.turb_ndt > 0 ? c->p.turb_ndt : 100);
     return refresh_btab_any(c, s);
 }
 
@@ -548,6 +610,426 @@ int gmt_ic_turbulent(gmt_ctx* c, void* u, double rho0, double p0, double bx0, do
     cudaFree(m);
     cudaFree(bt);
     return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_ic_turbulent");
+}
+
+// ------------------------------------------------------------------------------------------
+// device-resident time loop (gmt_run)
+// ------------------------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+LoopConst loop_const_of(const gmt_params& p, double alpha, double beta, double sigma0, int flags) {
+    LoopConst C{};
+    C.courant = p.courant;
+    C.dx = p.boxlen / p.nx;
+    C.boxlen = p.boxlen;
+    C.cp_coef = p.glm_cp_coef;
+    C.glm_ch_scale = p.glm_ch_scale;
+    C.turb_T = p.turb_T;
+    C.dtf = p.turb_T / (p.turb_ndt > 0 ? p.turb_ndt : 100);
+    C.alpha = alpha;
+    C.beta = beta;
+    C.sigma0 = sigma0;
+    C.ch_max_signal = (flags & GMT_RUN_CH_MAXSIGNAL) ? 1 : 0;
+    C.do_turb = (flags & GMT_RUN_FORCING) ? 1 : 0;
+    C.seed = p.turb_seed;
+    return C;
+}
+
+template <class R>
+cudaError_t run_enqueue(gmt_ctx* c, const void* src, void* dst, int flags, cudaStream_t s) {
+    const gmt_params& p = c->p;
+    tick_kernel<<<1, 32, 0, s>>>(c->loop, c->loopc, c->cfl, 1);
+    if (flags & GMT_RUN_FORCING) {
+        ou_cond_kernel<<<1, 64, 0, s>>>(c->modes, c->loop, c->loopc, c->mode_k_dev);
+        btab_cond_kernel<R><<<dim3((p.ny * p.nz + 255) / 256, 1), 256, 0, s>>>((const BoxTables<R>*)c->bt, c->loop,
+                                                                              c->mode_k_dev);
+    }
+    cudaError_t e = cudaMemsetAsync(c->cfl, 0, 2 * sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    UnsplitArgs<R> A;
+    A.u = cplanes<R>(src, c->n);
+    A.o = planes<R>(dst, c->n);
+    A.nx = p.nx; A.ny = p.ny; A.nz = p.nz;
+    A.ox = c->ox; A.oy = c->oy; A.lz = c->lz;
+    A.dt = A.dtdx = A.ch = A.glm_fac = A.ramp = R(0);
+    A.K = consts_of<R>(p);
+    A.iflo = p.iflo; A.use_llf = p.riemann == GMT_RIEMANN_LLF; A.do_turb = (flags & GMT_RUN_FORCING) ? 1 : 0;
+    A.btab = A.do_turb ? static_cast<const R*>(c->btab) : nullptr;
+    A.trigx = static_cast<const R*>(c->trig[0]);
+    A.cfl_out = c->cfl;
+    A.err = c->err;
+    A.dx = (R)(p.boxlen / p.nx);
+    A.dparams = reinterpret_cast<const double*>(c->loop);
+    int riem = p.riemann == GMT_RIEMANN_LLF ? GMT_RIEMANN_HLLD : p.riemann;
+    return launch_unsplit(A, p.recon, riem, s);
+}
+
+cudaError_t run_enqueue_any(gmt_ctx* c, const void* src, void* dst, int flags, cudaStream_t s) {
+    return c->esize == 8 ? run_enqueue<double>(c, src, dst, flags, s) : run_enqueue<float>(c, src, dst, flags, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gmt_run(gmt_ctx* c, void* u, void* w, int32_t nsteps, double t0, double t_end, int32_t flags, void* stream,
+            double* t_out, int32_t* which) {
+    if (!c || !u || !w || u == w || nsteps < 0) return fail(GMT_ERR_ARG, "gmt_run: invalid arguments");
+    if (c->p.scheme != GMT_SCHEME_UNSPLIT) return fail(GMT_ERR_UNSUPPORTED, "gmt_run: unsplit scheme only");
+    if (!(t_end >= t0)) return fail(GMT_ERR_ARG, "gmt_run: t_end < t0");
+    cudaStream_t s = (cudaStream_t)stream;
+    LoopState S{};
+    S.dt = 0.0; S.ch = 1.0; S.glm_fac = 1.0; S.ramp = 0.0;
+    S.t = t0; S.t_end = t_end; S.next_time = c->next_time; S.counter = c->counter;
+    LoopConst C = loop_const_of(c->p, c->alpha, c->beta, c->sigma0, flags);
+    GMT_CUDA(cudaMemcpyAsync(c->loop, &S, sizeof(S), cudaMemcpyHostToDevice, s));
+    GMT_CUDA(cudaMemcpyAsync(c->loopc, &C, sizeof(C), cudaMemcpyHostToDevice, s));
+    int rc = gmt_cfl_async(c, u, stream);   // CFL of the initial state; later steps fuse it
+    if (rc) return rc;
+    const int pairs = nsteps / 2;
+    if ((flags & GMT_RUN_GRAPH) && pairs > 0) {
+        cudaGraphExec_t exec = nullptr;
+        for (auto& g : c->graphs)
+            if (g.u == u && g.w == w && g.flags == flags) exec = g.exec;
+        if (!exec) {
+            cudaGraph_t graph;
+            GMT_CUDA(cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeRelaxed));
+            cudaError_t e1 = run_enqueue_any(c, u, w, flags, c->cap);
+            cudaError_t e2 = run_enqueue_any(c, w, u, flags, c->cap);
+            cudaError_t e3 = cudaStreamEndCapture(c->cap, &graph);
+            if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+                cudaGetLastError();
+                return cuda_fail(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3), "gmt_run capture");
+            }
+            cudaError_t e4 = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e4 != cudaSuccess) return cuda_fail(e4, "gmt_run instantiate");
+            if (c->graphs.size() >= 8) {
+                cudaGraphExecDestroy(c->graphs.front().exec);
+                c->graphs.erase(c->graphs.begin());
+            }
+            c->graphs.push_back({u, w, flags, exec});
+        }
+        for (int i = 0; i < pairs; ++i) GMT_CUDA(cudaGraphLaunch(exec, s));
+    } else {
+        for (int i = 0; i < pairs; ++i) {
+            GMT_CUDA(run_enqueue_any(c, u, w, flags, s));
+            GMT_CUDA(run_enqueue_any(c, w, u, flags, s));
+        }
+    }
+    if (nsteps & 1) GMT_CUDA(run_enqueue_any(c, u, w, flags, s));
+    int herr = 0;
+    GMT_CUDA(cudaMemcpyAsync(&S, c->loop, sizeof(S), cudaMemcpyDeviceToHost, s));
+    GMT_CUDA(cudaMemcpyAsync(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GMT_CUDA(cudaStreamSynchronize(s));
+    c->next_time = S.next_time;
+    c->counter = S.counter;
+    if (t_out) *t_out = S.t;
+    if (which) *which = nsteps & 1;
+    if (herr) {
+        cudaMemset(c->err, 0, sizeof(int));
+        return fail(GMT_ERR_TIMEOUT, "gmt_run: a step kernel abandoned a bounded wait");
+    }
+    if (S.status) return fail(GMT_ERR_STATE, "gmt_run: CFL maximum not positive and finite (invalid state)");
+    return GMT_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// ensemble
+// ------------------------------------------------------------------------------------------
+}  // extern "C"
+
+struct gmt_ensemble {
+    gmt_params p;
+    int nbox = 0;
+    int esize = 4;
+    int nsm = 148;
+    std::vector<int> n;
+    std::vector<double> amp;
+    std::vector<uint32_t> seed;
+    LoopState* loop = nullptr;       // [nbox]
+    LoopConst* loopc = nullptr;      // [nbox]
+    unsigned long long* cfl = nullptr;  // [2 nbox]
+    double* modes = nullptr;         // [nbox][61][3][2]
+    std::vector<void*> btab, trig;   // per box: row table; trig x, y, z
+    void* bt = nullptr;              // BoxTables<R>[nbox]
+    void* args = nullptr;            // UnsplitArgs<R>[2][nbox]
+    EnsItem* items = nullptr;
+    int nitems = 0;
+    unsigned* queue = nullptr;       // [2] one counter per parity
+    int* err = nullptr;
+    const int* mode_k_dev = nullptr;
+    cudaStream_t cap = nullptr;
+    std::vector<const void*> bound_u, bound_w;
+    cudaGraphExec_t exec = nullptr;
+    int exec_flags = -1;
+    int rows_max = 0;
+    std::vector<double> alpha, beta, sigma0;
+};
+
+namespace {
+
+template <class R> int ens_bind(gmt_ensemble* E, void* const* u, void* const* w, int flags) {
+    std::vector<UnsplitArgs<R>> A(2 * E->nbox);
+    for (int par = 0; par < 2; ++par)
+        for (int b = 0; b < E->nbox; ++b) {
+            UnsplitArgs<R>& a = A[par * E->nbox + b];
+            const int n = E->n[b];
+            const size_t cells = (size_t)n * n * n;
+            a.u = cplanes<R>(par == 0 ? u[b] : w[b], cells);
+            a.o = planes<R>(par == 0 ? w[b] : u[b], cells);
+            a.nx = a.ny = a.nz = n;
+            a.ox = 16; a.oy = 16; a.lz = 16;
+            a.dt = a.dtdx = a.ch = a.glm_fac = a.ramp = R(0);
+            a.K = consts_of<R>(E->p);
+            a.iflo = E->p.iflo; a.use_llf = E->p.riemann == GMT_RIEMANN_LLF;
+            a.do_turb = (flags & GMT_RUN_FORCING) ? 1 : 0;
+            a.btab = a.do_turb ? static_cast<const R*>(E->btab[b]) : nullptr;
+            a.trigx = static_cast<const R*>(E->trig[3 * b]);
+            a.cfl_out = E->cfl + 2 * b;
+            a.err = E->err;
+            a.dx = (R)(E->p.boxlen / n);
+            a.dparams = reinterpret_cast<const double*>(E->loop + b);
+        }
+    cudaError_t e = cudaMemcpy(E->args, A.data(), A.size() * sizeof(UnsplitArgs<R>), cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "ensemble bind");
+}
+
+template <class R> cudaError_t ens_enqueue(gmt_ensemble* E, int par, int flags, cudaStream_t s) {
+    tick_kernel<<<(E->nbox + 63) / 64, 64, 0, s>>>(E->loop, E->loopc, E->cfl, E->nbox);
+    if (flags & GMT_RUN_FORCING) {
+        ou_cond_kernel<<<E->nbox, 64, 0, s>>>(E->modes, E->loop, E->loopc, E->mode_k_dev);
+        btab_cond_kernel<R><<<dim3((E->rows_max + 255) / 256, E->nbox), 256, 0, s>>>((const BoxTables<R>*)E->bt, E->loop,
+                                                                                     E->mode_k_dev);
+    }
+    cudaError_t e = cudaMemsetAsync(E->cfl, 0, 2 * E->nbox * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(E->queue + par, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    const UnsplitArgs<R>* args = static_cast<const UnsplitArgs<R>*>(E->args) + par * E->nbox;
+    int riem = E->p.riemann == GMT_RIEMANN_LLF ? GMT_RIEMANN_HLLD : E->p.riemann;
+    return launch_ensemble(args, E->items, E->nitems, E->queue + par, E->p.recon, riem, E->nsm, s);
+}
+
+cudaError_t ens_enqueue_any(gmt_ensemble* E, int par, int flags, cudaStream_t s) {
+    return E->esize == 8 ? ens_enqueue<double>(E, par, flags, s) : ens_enqueue<float>(E, par, flags, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gmt_ensemble_destroy(gmt_ensemble* E) {
+    if (!E) return GMT_OK;
+    if (E->exec) cudaGraphExecDestroy(E->exec);
+    if (E->cap) cudaStreamDestroy(E->cap);
+    cudaFree(E->loop);
+    cudaFree(E->loopc);
+    cudaFree(E->cfl);
+    cudaFree(E->modes);
+    for (void* x : E->btab) cudaFree(x);
+    for (void* x : E->trig) cudaFree(x);
+    cudaFree(E->bt);
+    cudaFree(E->args);
+    cudaFree(E->items);
+    cudaFree(E->queue);
+    cudaFree(E->err);
+    delete E;
+    return GMT_OK;
+}
+
+int gmt_ensemble_create(const gmt_params* base, int32_t nbox, const int32_t* n, const double* amp,
+                        const uint32_t* seeds, gmt_ensemble** out) {
+    if (!base || !n || !out || nbox < 1) return fail(GMT_ERR_ARG, "gmt_ensemble_create: invalid arguments");
+    *out = nullptr;
+    if (base->abi_version != GMT_ABI_VERSION) return fail(GMT_ERR_ARG, "gmt_ensemble_create: abi_version mismatch");
+    if (base->scheme != GMT_SCHEME_UNSPLIT) return fail(GMT_ERR_UNSUPPORTED, "gmt_ensemble_create: unsplit scheme only");
+    if (!((base->recon == GMT_RECON_MC && (base->riemann == GMT_RIEMANN_HLLD || base->riemann == GMT_RIEMANN_HLL ||
+                                          base->riemann == GMT_RIEMANN_LLF)) ||
+          (base->recon == GMT_RECON_PPM && base->riemann == GMT_RIEMANN_HLL)))
+        return fail(GMT_ERR_UNSUPPORTED, "gmt_ensemble_create: built for PLM-MC with HLLD/HLL/LLF and PPM with HLL");
+    if (base->dtype != GMT_F32 && base->dtype != GMT_F64) return fail(GMT_ERR_ARG, "gmt_ensemble_create: bad dtype");
+    for (int b = 0; b < nbox; ++b)
+        if (n[b] < 16 || n[b] % 16 != 0)
+            return fail(GMT_ERR_ARG, "gmt_ensemble_create: every box size must be a positive multiple of 16");
+    std::call_once(g_mode_once, [] { g_mode_err = upload_mode_table(); });
+    if (g_mode_err != cudaSuccess) return cuda_fail(g_mode_err, "mode table");
+    {
+        cudaError_t e = base->dtype == GMT_F64 ? unsplit_prepare_f64() : unsplit_prepare_f32();
+        if (e != cudaSuccess) return cuda_fail(e, "kernel attributes");
+    }
+    gmt_ensemble* E = new gmt_ensemble();
+    E->p = *base;
+    E->nbox = nbox;
+    E->esize = base->dtype == GMT_F64 ? 8 : 4;
+    E->n.assign(n, n + nbox);
+    E->amp.resize(nbox);
+    E->seed.resize(nbox);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&E->nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void** ptr, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(ptr, bytes);
+    };
+    A((void**)&E->loop, nbox * sizeof(LoopState));
+    A((void**)&E->loopc, nbox * sizeof(LoopConst));
+    A((void**)&E->cfl, 2 * nbox * sizeof(unsigned long long));
+    A((void**)&E->modes, (size_t)nbox * NMODES * 6 * sizeof(double));
+    A(&E->bt, nbox * sizeof(BoxTables<double>));
+    A(&E->args, 2 * nbox * sizeof(UnsplitArgs<double>));
+    A((void**)&E->queue, 2 * sizeof(unsigned));
+    A((void**)&E->err, sizeof(int));
+    E->btab.assign(nbox, nullptr);
+    E->trig.assign(3 * nbox, nullptr);
+    for (int b = 0; b < nbox; ++b) {
+        A(&E->btab[b], (size_t)n[b] * n[b] * 24 * E->esize);
+        for (int a = 0; a < 3; ++a) A(&E->trig[3 * b + a], (size_t)8 * n[b] * E->esize);
+        E->rows_max = std::max(E->rows_max, n[b] * n[b]);
+    }
+    // work items: biggest boxes first, 16x16 tiles x 16-plane chunks
+    std::vector<int> order(nbox);
+    for (int b = 0; b < nbox; ++b) order[b] = b;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
+    std::vector<EnsItem> items;
+    for (int b : order)
+        for (int bz = 0; bz < n[b] / 16; ++bz)
+            for (int by = 0; by < n[b] / 16; ++by)
+                for (int bx = 0; bx < n[b] / 16; ++bx) items.push_back({b, bx, by, bz});
+    E->nitems = (int)items.size();
+    A((void**)&E->items, items.size() * sizeof(EnsItem));
+    if (e == cudaSuccess) e = cudaMemcpy(E->items, items.data(), items.size() * sizeof(EnsItem), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(E->err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(E->modes, 0, (size_t)nbox * NMODES * 6 * sizeof(double));
+    if (e == cudaSuccess) e = mode_table_device(&E->mode_k_dev);
+    // trig tables, forcing constants, loop records, box tables
+    int nd = base->turb_ndt > 0 ? base->turb_ndt : 100;
+    double dtf = base->turb_T / nd;
+    double alpha = 1.0 - dtf / base->turb_T, beta = std::sqrt(2.0 * dtf / base->turb_T);
+    std::vector<LoopState> S(nbox);
+    std::vector<LoopConst> Cs(nbox);
+    std::vector<BoxTables<double>> Td(nbox);
+    std::vector<BoxTables<float>> Tf(nbox);
+    for (int b = 0; b < nbox && e == cudaSuccess; ++b) {
+        std::vector<double> t = trig_table(n[b]);
+        for (int a = 0; a < 3 && e == cudaSuccess; ++a) {
+            if (E->esize == 8) {
+                e = cudaMemcpy(E->trig[3 * b + a], t.data(), t.size() * 8, cudaMemcpyHostToDevice);
+            } else {
+                std::vector<float> f(t.begin(), t.end());
+                e = cudaMemcpy(E->trig[3 * b + a], f.data(), f.size() * 4, cudaMemcpyHostToDevice);
+            }
+        }
+        E->amp[b] = amp ? amp[b] : base->turb_amp;
+        E->seed[b] = seeds ? seeds[b] : base->turb_seed + (uint32_t)b;
+        gmt_params pb = *base;
+        pb.nx = pb.ny = pb.nz = n[b];
+        pb.turb_seed = E->seed[b];
+        Cs[b] = loop_const_of(pb, alpha, beta, forcing_sigma0(E->amp[b], alpha, beta),
+                              GMT_RUN_CH_MAXSIGNAL | GMT_RUN_FORCING);
+        S[b] = LoopState{};
+        S[b].ch = 1.0; S[b].glm_fac = 1.0;
+        S[b].t = 0.0; S[b].t_end = 0.0; S[b].next_time = 0.0; S[b].counter = 0;
+        const double* mb = E->modes + (size_t)b * NMODES * 6;
+        Td[b] = BoxTables<double>{mb, (const double*)E->trig[3 * b + 1], (const double*)E->trig[3 * b + 2],
+                                  (double*)E->btab[b], n[b], n[b]};
+        Tf[b] = BoxTables<float>{mb, (const float*)E->trig[3 * b + 1], (const float*)E->trig[3 * b + 2],
+                                 (float*)E->btab[b], n[b], n[b]};
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(E->loop, S.data(), nbox * sizeof(LoopState), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(E->loopc, Cs.data(), nbox * sizeof(LoopConst), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = E->esize == 8 ? cudaMemcpy(E->bt, Td.data(), nbox * sizeof(Td[0]), cudaMemcpyHostToDevice)
+                          : cudaMemcpy(E->bt, Tf.data(), nbox * sizeof(Tf[0]), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        gmt_ensemble_destroy(E);
+        return cuda_fail(e, "gmt_ensemble_create");
+    }
+    *out = E;
+    return GMT_OK;
+}
+
+int gmt_ensemble_run(gmt_ensemble* E, void* const* u, void* const* w, int32_t nsteps, double t_end, int32_t flags,
+                     void* stream, double* t_out) {
+    if (!E || !u || !w || nsteps < 0) return fail(GMT_ERR_ARG, "gmt_ensemble_run: invalid arguments");
+    for (int b = 0; b < E->nbox; ++b)
+        if (!u[b] || !w[b] || u[b] == w[b]) return fail(GMT_ERR_ARG, "gmt_ensemble_run: bad state pointers");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = E->nbox;
+    bool rebind = (int)E->bound_u.size() != nb || E->exec_flags != flags;
+    for (int b = 0; !rebind && b < nb; ++b) rebind = E->bound_u[b] != u[b] || E->bound_w[b] != w[b];
+    if (rebind) {
+        GMT_CUDA(cudaStreamSynchronize(s));
+        int rc = E->esize == 8 ? ens_bind<double>(E, u, w, flags) : ens_bind<float>(E, u, w, flags);
+        if (rc) return rc;
+        E->bound_u.assign(u, u + nb);
+        E->bound_w.assign(w, w + nb);
+        if (E->exec) { cudaGraphExecDestroy(E->exec); E->exec = nullptr; }
+        E->exec_flags = flags;
+        // per-run flags live in the loop constants
+        std::vector<LoopConst> Cs(nb);
+        GMT_CUDA(cudaMemcpy(Cs.data(), E->loopc, nb * sizeof(LoopConst), cudaMemcpyDeviceToHost));
+        for (auto& C : Cs) {
+            C.ch_max_signal = (flags & GMT_RUN_CH_MAXSIGNAL) ? 1 : 0;
+            C.do_turb = (flags & GMT_RUN_FORCING) ? 1 : 0;
+        }
+        GMT_CUDA(cudaMemcpy(E->loopc, Cs.data(), nb * sizeof(LoopConst), cudaMemcpyHostToDevice));
+    }
+    // t_end of every box, then the CFL maxima of the initial states
+    std::vector<LoopState> S(nb);
+    GMT_CUDA(cudaMemcpyAsync(S.data(), E->loop, nb * sizeof(LoopState), cudaMemcpyDeviceToHost, s));
+    GMT_CUDA(cudaStreamSynchronize(s));
+    for (auto& x : S) x.t_end = t_end;
+    GMT_CUDA(cudaMemcpyAsync(E->loop, S.data(), nb * sizeof(LoopState), cudaMemcpyHostToDevice, s));
+    for (int b = 0; b < nb; ++b) {
+        const size_t cells = (size_t)E->n[b] * E->n[b] * E->n[b];
+        cudaError_t e = E->esize == 8
+                            ? launch_cfl<double>(cplanes<double>(u[b], cells), cells, consts_of<double>(E->p), E->cfl + 2 * b, s)
+                            : launch_cfl<float>(cplanes<float>(u[b], cells), cells, consts_of<float>(E->p), E->cfl + 2 * b, s);
+        if (e != cudaSuccess) return cuda_fail(e, "ensemble cfl");
+    }
+    const int pairs = nsteps / 2;
+    if ((flags & GMT_RUN_GRAPH) && pairs > 0) {
+        if (!E->exec) {
+            cudaGraph_t graph;
+            GMT_CUDA(cudaStreamBeginCapture(E->cap, cudaStreamCaptureModeRelaxed));
+            cudaError_t e1 = ens_enqueue_any(E, 0, flags, E->cap);
+            cudaError_t e2 = ens_enqueue_any(E, 1, flags, E->cap);
+            cudaError_t e3 = cudaStreamEndCapture(E->cap, &graph);
+            if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+                cudaGetLastError();
+                return cuda_fail(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3), "ensemble capture");
+            }
+            cudaError_t e4 = cudaGraphInstantiate(&E->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e4 != cudaSuccess) return cuda_fail(e4, "ensemble instantiate");
+        }
+        for (int i = 0; i < pairs; ++i) GMT_CUDA(cudaGraphLaunch(E->exec, s));
+    } else {
+        for (int i = 0; i < pairs; ++i) {
+            GMT_CUDA(ens_enqueue_any(E, 0, flags, s));
+            GMT_CUDA(ens_enqueue_any(E, 1, flags, s));
+        }
+    }
+    if (nsteps & 1) GMT_CUDA(ens_enqueue_any(E, 0, flags, s));
+    int herr = 0;
+    GMT_CUDA(cudaMemcpyAsync(S.data(), E->loop, nb * sizeof(LoopState), cudaMemcpyDeviceToHost, s));
+    GMT_CUDA(cudaMemcpyAsync(&herr, E->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GMT_CUDA(cudaStreamSynchronize(s));
+    int bad = 0;
+    for (int b = 0; b < nb; ++b) {
+        if (t_out) t_out[b] = S[b].t;
+        bad |= S[b].status;
+    }
+    if (herr) {
+        cudaMemset(E->err, 0, sizeof(int));
+        return fail(GMT_ERR_TIMEOUT, "gmt_ensemble_run: a step kernel abandoned a bounded wait");
+    }
+    if (bad) return fail(GMT_ERR_STATE, "gmt_ensemble_run: a box has no positive finite CFL maximum");
+    return GMT_OK;
 }
 
 // ------------------------------------------------------------------------------------------

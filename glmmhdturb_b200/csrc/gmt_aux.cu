@@ -192,6 +192,13 @@ cudaError_t launch_ct_divb(const CPlanes8<R>& q, int nx, int ny, int nz, double 
 // ------------------------------------------------------------------------------------------
 // forcing
 // ------------------------------------------------------------------------------------------
+cudaError_t mode_table_device(const int** ptr) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, c_mode_k);
+    *ptr = static_cast<const int*>(p);
+    return e;
+}
+
 cudaError_t upload_mode_table() {
     int k[NMODES * 3];
     int n = 0;
@@ -209,51 +216,12 @@ cudaError_t upload_mode_table() {
     return cudaMemcpyToSymbol(c_mode_k, k, sizeof(k));
 }
 
-// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11)
-__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
-        uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
-        uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
-        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
-    }
-}
-
 __global__ void ou_update_kernel(double* modes, uint32_t seed, uint32_t counter, double alpha, double beta,
                                  double sigma0) {
     int q = threadIdx.x;
     if (q >= NMODES) return;
-    uint32_t r[8] = {counter, (uint32_t)q, 0u, 0u, counter, (uint32_t)q, 1u, 0u};
-    philox4x32_10(r, seed, 0x9E3779B9u);
-    philox4x32_10(r + 4, seed, 0x9E3779B9u);
-    const double twopi = 6.283185307179586476925286766559;
-    double z[6];
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-        double u1 = ((double)r[2 * b] + 0.5) * 2.3283064365386962890625e-10;
-        double u2 = ((double)r[2 * b + 1] + 0.5) * 2.3283064365386962890625e-10;
-        double rr = sqrt(-2.0 * log(u1));
-        double th = twopi * u2;
-        z[2 * b] = rr * cos(th);
-        z[2 * b + 1] = rr * sin(th);
-    }
-    double kx = c_mode_k[3 * q], ky = c_mode_k[3 * q + 1], kz = c_mode_k[3 * q + 2];
-    double kk = sqrt(kx * kx + ky * ky + kz * kz);
-    double ux = kx / kk, uy = ky / kk, uz = kz / kk;
-    double sig = sigma0 / kk;
-    double kr = ux * z[0] + uy * z[2] + uz * z[4];
-    double ki = ux * z[1] + uy * z[3] + uz * z[5];
-    double uu[3] = {ux, uy, uz};
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        double pr = z[2 * c] - uu[c] * kr;
-        double pi = z[2 * c + 1] - uu[c] * ki;
-        double* m = modes + (q * 3 + c) * 2;
-        m[0] = alpha * m[0] + beta * sig * pr;
-        m[1] = alpha * m[1] + beta * sig * pi;
-    }
+    ou_mode_update(modes, q, c_mode_k[3 * q], c_mode_k[3 * q + 1], c_mode_k[3 * q + 2], seed, counter, alpha, beta,
+                   sigma0);
 }
 
 cudaError_t launch_ou_update(double* modes, uint32_t seed, uint32_t counter, double alpha, double beta, double sigma0,
@@ -268,31 +236,7 @@ __global__ void __launch_bounds__(256) btab_kernel(const double* modes, const R*
                                                    R* btab) {
     int row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= ny * nz) return;
-    int j = row % ny, k = row / ny;
-    R* out = btab + (size_t)row * 24;
-    int q = 0;
-    for (int kx = 0; kx <= 3; ++kx) {
-        R Br[3] = {R(0), R(0), R(0)}, Bi[3] = {R(0), R(0), R(0)};
-        while (q < NMODES && c_mode_k[3 * q] == kx) {
-            int ky = c_mode_k[3 * q + 1], kz = c_mode_k[3 * q + 2];
-            int ay = ky < 0 ? -ky : ky, az = kz < 0 ? -kz : kz;
-            R eyr = trigy[(2 * ay) * ny + j], eyi = trigy[(2 * ay + 1) * ny + j];
-            R ezr = trigz[(2 * az) * nz + k], ezi = trigz[(2 * az + 1) * nz + k];
-            if (ky < 0) eyi = -eyi;
-            if (kz < 0) ezi = -ezi;
-            R er = eyr * ezr - eyi * ezi;
-            R ei = eyr * ezi + eyi * ezr;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                R ar = (R)modes[(q * 3 + c) * 2], ai = (R)modes[(q * 3 + c) * 2 + 1];
-                Br[c] = Br[c] + (ar * er - ai * ei);
-                Bi[c] = Bi[c] + (ar * ei + ai * er);
-            }
-            ++q;
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) { out[kx * 6 + 2 * c] = Br[c]; out[kx * 6 + 2 * c + 1] = Bi[c]; }
-    }
+    btab_row(modes, c_mode_k, trigy, trigz, ny, nz, row % ny, row / ny, btab + (size_t)row * 24);
 }
 
 template <class R>

@@ -31,7 +31,27 @@ template <class R> struct UnsplitArgs {
     const R* trigx;        // [4 m][2 cos|sin][nx]
     unsigned long long* cfl_out;  // [2] bits of non-negative doubles (max ctot, max signal) or null
     int* err;              // set to 1 when a bounded wait gives up (never expected)
+    R dx;                  // cell size (dt/dx of device-supplied steps)
+    const double* dparams; // if set: dt, ch, glm_fac, ramp of this step read from device memory
 };
+
+// step values of one box, from the kernel arguments or from device memory
+template <class R> struct StepVals {
+    R dt, dtdx, ch, glm_fac, ramp;
+};
+template <class R> __device__ __forceinline__ StepVals<R> step_vals(const UnsplitArgs<R>& A) {
+    StepVals<R> V;
+    if (A.dparams) {
+        V.dt = (R)A.dparams[0];
+        V.dtdx = V.dt / A.dx;
+        V.ch = (R)A.dparams[1];
+        V.glm_fac = (R)A.dparams[2];
+        V.ramp = (R)A.dparams[3];
+    } else {
+        V.dt = A.dt; V.dtdx = A.dtdx; V.ch = A.ch; V.glm_fac = A.glm_fac; V.ramp = A.ramp;
+    }
+    return V;
+}
 
 // cp.async 4-byte global -> shared copy (L1-allocating), plus group commit / wait.
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
@@ -50,6 +70,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
     unsigned s = (unsigned)__cvta_generic_to_shared(bar);
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(s), "r"(count));
+}
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(s) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive_cp_async(uint64_t* bar) {
     unsigned s = (unsigned)__cvta_generic_to_shared(bar);
@@ -105,6 +129,83 @@ __device__ __forceinline__ void cfl_speeds(const Q9<R>& c, const Consts<R>& K, R
     R sz = rabs(q.v[3]) + fast_speed(q, K.gamma, q.v[7]);
     ctot = sx + sy + sz;
     smax = rmax(rmax(sx, sy), sz);
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11)
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+
+// One OU step of mode q with wavevector (kx,ky,kz): ahat <- alpha*ahat + beta*sigma_k*P_k(xi),
+// xi = 6 normals from Philox(counter = {counter, q, 0|1, 0}, key = {seed, 0x9E3779B9}) + Box-Muller,
+// P_k the solenoidal projector, sigma_k = sigma0/|k| (modes: [61][3][2] doubles)
+__device__ __forceinline__ void ou_mode_update(double* modes, int q, int ikx, int iky, int ikz, uint32_t seed,
+                                               uint32_t counter, double alpha, double beta, double sigma0) {
+    uint32_t r[8] = {counter, (uint32_t)q, 0u, 0u, counter, (uint32_t)q, 1u, 0u};
+    philox4x32_10(r, seed, 0x9E3779B9u);
+    philox4x32_10(r + 4, seed, 0x9E3779B9u);
+    const double twopi = 6.283185307179586476925286766559;
+    double z[6];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        double u1 = ((double)r[2 * b] + 0.5) * 2.3283064365386962890625e-10;
+        double u2 = ((double)r[2 * b + 1] + 0.5) * 2.3283064365386962890625e-10;
+        double rr = sqrt(-2.0 * log(u1));
+        double th = twopi * u2;
+        z[2 * b] = rr * cos(th);
+        z[2 * b + 1] = rr * sin(th);
+    }
+    double kx = ikx, ky = iky, kz = ikz;
+    double kk = sqrt(kx * kx + ky * ky + kz * kz);
+    double ux = kx / kk, uy = ky / kk, uz = kz / kk;
+    double sig = sigma0 / kk;
+    double kr = ux * z[0] + uy * z[2] + uz * z[4];
+    double ki = ux * z[1] + uy * z[3] + uz * z[5];
+    double uu[3] = {ux, uy, uz};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double pr = z[2 * c] - uu[c] * kr;
+        double pi = z[2 * c + 1] - uu[c] * ki;
+        double* m = modes + (q * 3 + c) * 2;
+        m[0] = alpha * m[0] + beta * sig * pr;
+        m[1] = alpha * m[1] + beta * sig * pi;
+    }
+}
+
+// per-row mode table B[kx][c] of row (j, k) (same summation order as the oracle's Forcer::accel)
+template <class R>
+__device__ __forceinline__ void btab_row(const double* modes, const int* mode_k, const R* trigy, const R* trigz, int ny,
+                                         int nz, int j, int k, R* out) {
+    int q = 0;
+    for (int kx = 0; kx <= 3; ++kx) {
+        R Br[3] = {R(0), R(0), R(0)}, Bi[3] = {R(0), R(0), R(0)};
+        while (q < 61 && mode_k[3 * q] == kx) {
+            int ky = mode_k[3 * q + 1], kz = mode_k[3 * q + 2];
+            int ay = ky < 0 ? -ky : ky, az = kz < 0 ? -kz : kz;
+            R eyr = trigy[(2 * ay) * ny + j], eyi = trigy[(2 * ay + 1) * ny + j];
+            R ezr = trigz[(2 * az) * nz + k], ezi = trigz[(2 * az + 1) * nz + k];
+            if (ky < 0) eyi = -eyi;
+            if (kz < 0) ezi = -ezi;
+            R er = eyr * ezr - eyi * ezi;
+            R ei = eyr * ezi + eyi * ezr;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R ar = (R)modes[(q * 3 + c) * 2], ai = (R)modes[(q * 3 + c) * 2 + 1];
+                Br[c] = Br[c] + (ar * er - ai * ei);
+                Bi[c] = Bi[c] + (ar * ei + ai * er);
+            }
+            ++q;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { out[kx * 6 + 2 * c] = Br[c]; out[kx * 6 + 2 * c + 1] = Bi[c]; }
+    }
 }
 
 // forcing acceleration at one cell from the per-row table (same order as the oracle)

@@ -15,6 +15,13 @@ constexpr int NMODES = 61;
 cudaError_t launch_unsplit(const UnsplitArgs<float>& A, int recon, int riem, cudaStream_t s);
 cudaError_t launch_unsplit(const UnsplitArgs<double>& A, int recon, int riem, cudaStream_t s);
 int unsplit_max_threads(int dtype_bytes);
+cudaError_t unsplit_prepare_f32();   // shared-memory attributes of every step kernel
+cudaError_t unsplit_prepare_f64();
+struct EnsItem;
+cudaError_t launch_ensemble(const UnsplitArgs<float>* boxes, const EnsItem* items, int nitems, unsigned* queue,
+                            int recon, int riem, int nsm, cudaStream_t s);
+cudaError_t launch_ensemble(const UnsplitArgs<double>* boxes, const EnsItem* items, int nitems, unsigned* queue,
+                            int recon, int riem, int nsm, cudaStream_t s);
 size_t unsplit_smem(int dtype_bytes, int ox, int oy);
 int unsplit_regs(int dtype_bytes, int recon, int riem, int nthreads);
 
@@ -68,7 +75,11 @@ template <class R> cudaError_t launch_ct_ic_ot(const Planes8<R>& q, int nx, int 
 template <class R> cudaError_t launch_ic_turb(const Planes<R>& u, int nx, int ny, int nz, const R* btab,
                                              const R* trigx, double rho0, double p0, const double b0[3],
                                              double vscale, double bscale, double gamma, cudaStream_t s);
+size_t spectrum_scratch_bytes(int nx, int ny, int nz, int kmax);
+template <class R> cudaError_t launch_spectrum(const CPlanes<R>& u, int nx, int ny, int nz, int kmax, void* scratch,
+                                               double* E_host, cudaStream_t s);
 cudaError_t upload_mode_table();   // the 61 wavevectors into constant memory
+cudaError_t mode_table_device(const int** ptr);   // device address of that table
 void set_last_error(const std::string& msg);   // message returned by gmt_last_error() on this thread
 
 }  // namespace gmt

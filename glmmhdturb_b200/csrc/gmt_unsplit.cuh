@@ -75,7 +75,10 @@ __device__ __forceinline__ Q9<R> face_state(const Rec<R>& r, const R* __restrict
     } else {
         f = padd(r.mh, r.s[D], SIGN > 0 ? R(1) : R(-1));
     }
-    if (iflo && (f.v[0] < K.smallr || f.v[4] < K.pfl)) f = r.m0;
+    // revert an unphysical state to the cell value; the revert is rare, so the 9 selects are
+    // skipped when no lane of the warp needs them
+    const bool bad = iflo && (f.v[0] < K.smallr || f.v[4] < K.pfl);
+    if (__any_sync(__activemask(), bad) && bad) f = r.m0;
     return f;
 }
 
@@ -127,10 +130,13 @@ template <class R> __host__ __device__ inline size_t unsplit_smem_bytes(int ox, 
     return (27 * PN + 36 * RN + 9 * PN) * sizeof(R) + 40 * sizeof(double);
 }
 
-template <class R, int RECON, int RIEM, int MAXT, int MINB>
-__global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R> A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int OX = A.ox, OY = A.oy;
+// One tile (bx, by) x z-chunk bz of one box.  TOX, TOY > 0 fix the tile at compile time
+// (constant shared-memory offsets); 0 = runtime tile.  Used by the single-box kernel (one tile per
+// block) and by the ensemble kernel (a queue of tiles over many boxes).
+template <class R, int RECON, int RIEM, int TOX, int TOY>
+__device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const StepVals<R>& V, int bx, int by, int bz,
+                                             unsigned char* smem_raw) {
+    const int OX = TOX > 0 ? TOX : A.ox, OY = TOY > 0 ? TOY : A.oy;
     const int PW = OX + 4, PN = (OX + 4) * (OY + 4);
     const int RW = OX + 2, RN = (OX + 2) * (OY + 2);
     R* PR = reinterpret_cast<R*>(smem_raw);
@@ -140,11 +146,11 @@ __global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R
 
     const int tid = threadIdx.x, NT = OX * OY;
     const int tx = tid % OX, ty = tid / OX;
-    const int x0 = blockIdx.x * OX, y0 = blockIdx.y * OY;
-    const int z0 = blockIdx.z * A.lz, z1 = min(z0 + A.lz, A.nz);
+    const int x0 = bx * OX, y0 = by * OY;
+    const int z0 = bz * A.lz, z1 = min(z0 + A.lz, A.nz);
     const int nx = A.nx, ny = A.ny, nz = A.nz;
     const Consts<R> K = A.K;
-    const R dtdx = A.dtdx, ch = A.ch;
+    const R dtdx = V.dtdx, ch = V.ch;
     const bool turb = A.do_turb && A.btab != nullptr;
     const int nhelp = 2 * (OX + OY);
 
@@ -210,8 +216,8 @@ __global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R
 #pragma unroll
                     for (int v = 0; v < 9; ++v) q.v[v] = A.u.p[v][g] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
                     R ax = R(0), ay = R(0), az = R(0);
-                    if (turb) force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, A.ramp, ax, ay, az);
-                    finish_update(q, K, A.glm_fac, turb, ax, ay, az, A.dt);
+                    if (turb) force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
+                    finish_update(q, K, V.glm_fac, turb, ax, ay, az, V.dt);
 #pragma unroll
                     for (int v = 0; v < 9; ++v) A.o.p[v][g] = q.v[v];
                     if (A.cfl_out) {
@@ -276,11 +282,42 @@ __global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R
         }
         __syncthreads();
     }
+    if (tid == 0) mbar_inval(mbar);
     if (A.cfl_out) {
         block_max_atomic(cmax, A.cfl_out, red);
         __syncthreads();
         block_max_atomic(smax, A.cfl_out + 1, red);
     }
+}
+
+// A tile = (box, bx, by, bz) work item of the ensemble kernel.
+struct EnsItem { int box, bx, by, bz; };
+
+// Persistent ensemble step: each block takes work items from a global queue (one atomic per
+// item) until the queue is drained; every box has its own arguments, step values and CFL slot.
+template <class R, int RECON, int RIEM, int TOX, int TOY, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) ensemble_kernel(const UnsplitArgs<R>* __restrict__ boxes,
+                                                              const EnsItem* __restrict__ items, int nitems,
+                                                              unsigned* queue) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int item_s;
+    for (;;) {
+        if (threadIdx.x == 0) item_s = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int it = item_s;
+        __syncthreads();
+        if (it >= nitems) break;
+        const EnsItem w = items[it];
+        const UnsplitArgs<R> A = boxes[w.box];
+        unsplit_tile<R, RECON, RIEM, TOX, TOY>(A, step_vals(A), w.bx, w.by, w.bz, smem_raw);
+        __syncthreads();
+    }
+}
+
+template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0>
+__global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsplit_tile<R, RECON, RIEM, TOX, TOY>(A, step_vals(A), blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 }  // namespace gmt

@@ -7,5 +7,19 @@ cudaError_t launch_unsplit(const UnsplitArgs<double>& A, int recon, int riem, cu
     if (A.ox * A.oy > 256) return cudaErrorInvalidConfiguration;
     return unsplit_dispatch_t<double, 256, 1>(A, recon, riem, s);
 }
+cudaError_t unsplit_prepare_f64() {
+    cudaError_t e = unsplit_configure_all_t<double, 256, 1>();
+    for (int rc = 0; e == cudaSuccess && rc < 3; ++rc)
+        e = launch_ensemble((const UnsplitArgs<double>*)nullptr, nullptr, 0, nullptr, rc == 2 ? RECON_PPM : RECON_MC,
+                            rc == 0 ? RIEM_HLLD : RIEM_HLL, 1, 0);
+    return e;
+}
 int unsplit_regs_f64(int recon, int riem, int) { return unsplit_regs_of_t<double, 256, 1>(recon, riem); }
+cudaError_t launch_ensemble(const UnsplitArgs<double>* boxes, const EnsItem* items, int nitems, unsigned* queue,
+                            int recon, int riem, int nsm, cudaStream_t s) {
+    if (recon == RECON_MC && riem == RIEM_HLLD) return ensemble_go<double, RECON_MC, RIEM_HLLD>(boxes, items, nitems, queue, nsm, s);
+    if (recon == RECON_MC && riem == RIEM_HLL) return ensemble_go<double, RECON_MC, RIEM_HLL>(boxes, items, nitems, queue, nsm, s);
+    if (recon == RECON_PPM && riem == RIEM_HLL) return ensemble_go<double, RECON_PPM, RIEM_HLL>(boxes, items, nitems, queue, nsm, s);
+    return cudaErrorNotSupported;
+}
 }  // namespace gmt

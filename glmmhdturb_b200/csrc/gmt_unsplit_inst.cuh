@@ -7,16 +7,46 @@
 
 namespace gmt {
 
-template <class R, int RECON, int RIEM, int MAXT, int MINB>
-static cudaError_t unsplit_go(const UnsplitArgs<R>& A, cudaStream_t s) {
-    auto k = unsplit_kernel<R, RECON, RIEM, MAXT, MINB>;
-    static int configured[64] = {0};
+// Per device, once: allow the kernel up to 227 KB of dynamic shared memory.  Called for every
+// instantiation when a context is created, so that no attribute call happens during a stream
+// capture of the steps.
+template <class K> static cudaError_t configure_once(K k, int* configured) {
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 64 && !configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (dev >= 64 || configured[dev]) return cudaSuccess;
+    // the per-block limit covers static plus dynamic shared memory
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, k);
+    int optin = 227 * 1024;
+    if (e == cudaSuccess) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return e;
+    }
+    configured[dev] = 1;
+    return cudaSuccess;
+}
+
+template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0> struct UnsplitCfg {
+    static int configured[64];
+};
+template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX, int TOY>
+int UnsplitCfg<R, RECON, RIEM, MAXT, MINB, TOX, TOY>::configured[64] = {0};
+
+template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0>
+static cudaError_t unsplit_configure() {
+    return configure_once(unsplit_kernel<R, RECON, RIEM, MAXT, MINB, TOX, TOY>,
+                          UnsplitCfg<R, RECON, RIEM, MAXT, MINB, TOX, TOY>::configured);
+}
+
+template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0>
+static cudaError_t unsplit_go(const UnsplitArgs<R>& A, cudaStream_t s) {
+    auto k = unsplit_kernel<R, RECON, RIEM, MAXT, MINB, TOX, TOY>;
+    {
+        cudaError_t e = unsplit_configure<R, RECON, RIEM, MAXT, MINB, TOX, TOY>();
         if (e != cudaSuccess) return e;
-        configured[dev] = 1;
     }
     const int nt = A.ox * A.oy;
     if (nt > MAXT || nt < 1) return cudaErrorInvalidConfiguration;
@@ -36,6 +66,17 @@ static cudaError_t unsplit_dispatch_t(const UnsplitArgs<R>& A, int recon, int ri
     return cudaErrorInvalidValue;
 }
 
+template <class R, int MAXT, int MINB> static cudaError_t unsplit_configure_all_t() {
+    cudaError_t e = cudaSuccess;
+#define GMT_CASE(RC, RM) \
+    if (e == cudaSuccess) e = unsplit_configure<R, RC, RM, MAXT, MINB>();
+    GMT_CASE(RECON_MC, RIEM_HLLD) GMT_CASE(RECON_MC, RIEM_HLL) GMT_CASE(RECON_MC, RIEM_LLF_BOUND)
+    GMT_CASE(RECON_MINMOD, RIEM_HLLD) GMT_CASE(RECON_MINMOD, RIEM_HLL) GMT_CASE(RECON_MINMOD, RIEM_LLF_BOUND)
+    GMT_CASE(RECON_PPM, RIEM_HLLD) GMT_CASE(RECON_PPM, RIEM_HLL) GMT_CASE(RECON_PPM, RIEM_LLF_BOUND)
+#undef GMT_CASE
+    return e;
+}
+
 template <class R, int MAXT, int MINB> static int unsplit_regs_of_t(int recon, int riem) {
     cudaFuncAttributes fa{};
     cudaError_t e = cudaErrorInvalidValue;
@@ -48,4 +89,22 @@ template <class R, int MAXT, int MINB> static int unsplit_regs_of_t(int recon, i
     return e == cudaSuccess ? fa.numRegs : -1;
 }
 
+}  // namespace gmt
+
+namespace gmt {
+// ensemble launcher: 16x16 tiles, persistent grid of 2 blocks per SM
+template <class R, int RECON, int RIEM>
+static cudaError_t ensemble_go(const UnsplitArgs<R>* boxes, const EnsItem* items, int nitems, unsigned* queue,
+                               int nsm, cudaStream_t s) {
+    auto k = ensemble_kernel<R, RECON, RIEM, 16, 16, 256, 2>;
+    static int configured[64] = {0};
+    {
+        cudaError_t e = configure_once(k, configured);
+        if (e != cudaSuccess) return e;
+    }
+    if (nitems <= 0) return cudaSuccess;   // configure only
+    int nb = std::max(1, std::min(nitems, 2 * nsm));
+    k<<<nb, 256, unsplit_smem_bytes<R>(16, 16), s>>>(boxes, items, nitems, queue);
+    return cudaGetLastError();
+}
 }  // namespace gmt

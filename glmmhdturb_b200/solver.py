@@ -155,6 +155,13 @@ class Solver:
         check(lib().gmt_diagnostics(self._ctx, self._ptr(u), C.byref(d), _stream_handle(stream)))
         return {k: getattr(d, k) for k, _ in GmtDiag._fields_}
 
+    def ke_spectrum(self, u, kmax=8, stream=None) -> np.ndarray:
+        """Shell-binned kinetic-energy spectrum E(k), k = 0..kmax, of w = sqrt(rho) v (FP64)."""
+        out = np.zeros(kmax + 1)
+        check(lib().gmt_ke_spectrum(self._ctx, self._ptr(u), int(kmax), out.ctypes.data_as(C.POINTER(C.c_double)),
+                                    _stream_handle(stream)))
+        return out
+
     def ct_divb_max(self, q, stream=None) -> float:
         out = C.c_double()
         check(lib().gmt_ct_divb_max(self._ctx, self._ptr(q), C.byref(out), _stream_handle(stream)))
@@ -188,6 +195,18 @@ class Solver:
         check(lib().gmt_forcing_counter(self._ctx, C.byref(c)))
         return c.value
 
+    # ------------------------------------------------------------------ device-resident loop
+    def run(self, u, w, nsteps, t0=0.0, t_end=1e300, *, ch_max_signal=True, forcing=False, graph=True, stream=None):
+        """nsteps steps with dt, ch, glm_fac and the forcing cadence decided on the device (gmt_run);
+        returns (t reached, result tensor)."""
+        flags = ((_lib.RUN_CH_MAXSIGNAL if ch_max_signal else 0) | (_lib.RUN_FORCING if forcing else 0) |
+                 (_lib.RUN_GRAPH if graph else 0))
+        t = C.c_double()
+        which = C.c_int32()
+        check(lib().gmt_run(self._ctx, self._ptr(u), self._ptr(w), int(nsteps), float(t0), float(t_end), flags,
+                            _stream_handle(stream), C.byref(t), C.byref(which)))
+        return t.value, (w if which.value else u)
+
     # ------------------------------------------------------------------ initial conditions
     def ic_orszag_tang(self, u, stream=None):
         fn = lib().gmt_ct_ic_orszag_tang if self.scheme == "ct" else lib().gmt_ic_orszag_tang
@@ -201,3 +220,59 @@ class Solver:
         """Seeded synthetic turbulent state (gmt_ic_turbulent): rms Mach ~ `mach`, |dB| ~ `db`."""
         check(lib().gmt_ic_turbulent(self._ctx, self._ptr(u), rho0, p0, b0[0], b0[1], b0[2], mach, db, int(seed),
                                      _stream_handle(stream)))
+
+
+class Ensemble:
+    """Many periodic GLM boxes of different sizes advanced together: one persistent kernel per step
+    over a queue of 16x16x16 tiles of all boxes, every box with its own dt, forcing amplitude and
+    seed (gmt_ensemble_*)."""
+
+    def __init__(self, sizes, *, amps=None, seeds=None, dtype="f32", recon="mc", riemann="hlld", gamma=5.0 / 3.0,
+                 courant=0.3, turb_T=0.5, turb_ndt=100, **kw):
+        self.sizes = [int(n) for n in sizes]
+        self.dtype_name = dtype
+        self.code, self.torch_dtype = _DT[dtype]
+        p = GmtParams()
+        check(lib().gmt_params_init(C.byref(p), 16))
+        p.dtype = self.code
+        p.recon = _lib.RECON[recon]
+        p.riemann = _lib.RIEMANN[riemann]
+        p.gamma, p.courant, p.turb_T, p.turb_ndt = gamma, courant, turb_T, int(turb_ndt)
+        for k, v in kw.items():
+            setattr(p, k, v)
+        nb = len(self.sizes)
+        n_arr = (C.c_int32 * nb)(*self.sizes)
+        a_arr = (C.c_double * nb)(*(amps if amps is not None else [0.0] * nb))
+        s_arr = (C.c_uint32 * nb)(*(seeds if seeds is not None else list(range(nb))))
+        self._e = C.c_void_p()
+        check(lib().gmt_ensemble_create(C.byref(p), nb, n_arr, a_arr, s_arr, C.byref(self._e)))
+        self.device = torch.device("cuda", torch.cuda.current_device())
+
+    def alloc(self):
+        return [torch.empty((9, n, n, n), dtype=self.torch_dtype, device=self.device) for n in self.sizes]
+
+    def run(self, u, w, nsteps, t_end=1e300, *, ch_max_signal=True, forcing=True, graph=True, stream=None):
+        """nsteps ensemble steps; returns the list of times reached (result in u if nsteps is even)."""
+        nb = len(self.sizes)
+        for x, n in zip(list(u) + list(w), self.sizes + self.sizes):
+            if x.dtype != self.torch_dtype or x.numel() != 9 * n ** 3 or not x.is_contiguous():
+                raise ValueError("ensemble states must be contiguous 9 x n^3 tensors of the ensemble dtype")
+        ua = (C.c_void_p * nb)(*[x.data_ptr() for x in u])
+        wa = (C.c_void_p * nb)(*[x.data_ptr() for x in w])
+        t = (C.c_double * nb)()
+        flags = ((_lib.RUN_CH_MAXSIGNAL if ch_max_signal else 0) | (_lib.RUN_FORCING if forcing else 0) |
+                 (_lib.RUN_GRAPH if graph else 0))
+        check(lib().gmt_ensemble_run(self._e, C.cast(ua, C.c_void_p), C.cast(wa, C.c_void_p), int(nsteps),
+                                     float(t_end), flags, _stream_handle(stream), t))
+        return list(t)
+
+    def close(self):
+        if self._e:
+            lib().gmt_ensemble_destroy(self._e)
+            self._e = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

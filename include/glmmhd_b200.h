@@ -121,6 +121,39 @@ int gmt_compute_dt(gmt_ctx* ctx, const void* u, double* dt, void* stream);
 /* --- diagnostics (glmmhd_turb.jl:1996-2018), FP64, deterministic ------------------------- */
 int gmt_diagnostics(gmt_ctx* ctx, const void* u, gmt_diag* out, void* stream);
 
+/* --- device-resident time loop (no counterpart in the reference: its loop is host Julia,
+ *     glmmhd_turb.jl:2216-2230) ---------------------------------------------------------------- */
+enum { GMT_RUN_CH_MAXSIGNAL = 1, GMT_RUN_FORCING = 2, GMT_RUN_GRAPH = 4 };
+/* Run up to nsteps unsplit steps with every decision on the device: dt = courant*dx/max ctot from
+ * the CFL fused into the previous step, ch (the global max signal speed with GMT_RUN_CH_MAXSIGNAL,
+ * else courant*dx/dt/3*glm_ch_scale), glm_fac, the forcing ramp and the OU cadence
+ * (GMT_RUN_FORCING: advance when t >= next forcing time), dt clipped to the next forcing time and
+ * to t_end.  With GMT_RUN_GRAPH the two-step unit u->w->u is captured once into a CUDA graph and
+ * replayed.  Starts at t0 with the context's forcing state.  Returns the time reached (*t_out) and
+ * the buffer holding the result (*which: 0 = u, 1 = w); synchronous on return. */
+int gmt_run(gmt_ctx* ctx, void* u, void* w, int32_t nsteps, double t0, double t_end, int32_t flags, void* stream,
+            double* t_out, int32_t* which);
+
+/* --- batched ensemble: many periodic boxes of different sizes in one persistent launch per step -
+ * (no counterpart in the reference).  Every box: its own n^3 grid (n a multiple of 16), forcing
+ * amplitude and seed; the physics of `base`.  Each step: one tick per box, the conditional forcing
+ * updates, and one persistent kernel over a queue of 16x16x16 work items of all boxes. */
+typedef struct gmt_ensemble gmt_ensemble;
+int gmt_ensemble_create(const gmt_params* base, int32_t nbox, const int32_t* n, const double* turb_amp,
+                        const uint32_t* seeds, gmt_ensemble** out);
+int gmt_ensemble_destroy(gmt_ensemble* e);
+/* u[b], w[b]: device base pointers of box b's two 9-plane registers; the result is in u after an
+ * even number of steps, in w after an odd one; t_out[b] = time reached by box b */
+int gmt_ensemble_run(gmt_ensemble* e, void* const* u, void* const* w, int32_t nsteps, double t_end, int32_t flags,
+                     void* stream, double* t_out);
+
+/* --- turbulence statistics (no counterpart in the reference's step path; used by its turbulence
+ *     checks, GPU_SOLVER_OPTIMIZATION_PLAYBOOK.md:283-284) ------------------------------------ */
+/* shell-binned kinetic-energy spectrum of w = sqrt(rho) v: out[k] = 1/2 sum over the shell
+ * k-1/2 <= |k'| < k+1/2 of |w^(k')|^2 for k = 0..kmax (sum_k out[k] = mean kinetic energy density).
+ * FP64, deterministic; the context keeps the scratch of the largest kmax used.  Synchronous. */
+int gmt_ke_spectrum(gmt_ctx* ctx, const void* u, int32_t kmax, double* out, void* stream);
+
 /* --- diagnostics without allocation --------------------------------------------------------
  * No counterpart in the reference.  Same quantities as gmt_diagnostics for a 9-plane GLM state,
  * for callers that must not allocate device memory: a driver loop that cannot afford the device
