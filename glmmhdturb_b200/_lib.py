@@ -31,7 +31,7 @@ EXPORTS = (
     "gmt_forcing_reset", "gmt_forcing_advance", "gmt_forcing_set_modes", "gmt_forcing_get_modes",
     "gmt_forcing_counter", "gmt_ic_orszag_tang", "gmt_ic_uniform", "gmt_ic_turbulent", "gmt_ct_step", "gmt_ct_cfl_async",
     "gmt_ct_divb_max", "gmt_ct_ic_orszag_tang", "gmt_ke_spectrum", "gmt_run", "gmt_ensemble_create", "gmt_ensemble_destroy",
-    "gmt_ensemble_run", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
+    "gmt_ensemble_run", "gmt_ke_band_loss", "gmt_adjoint_step", "gmt_adjoint_amp_grad", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
     "march_set_glm", "march_set_gamma", "march_run_dev", "march_set_nx", "ct_run", "ct_regs", "ct_shmem",
 )
 
@@ -104,6 +104,9 @@ def lib():
             "gmt_ct_divb_max": ([vp, vp, C.POINTER(dbl), vp], C.c_int),
             "gmt_ct_ic_orszag_tang": ([vp, vp, vp], C.c_int),
             "gmt_ke_spectrum": ([vp, vp, i32, C.POINTER(dbl), vp], C.c_int),
+            "gmt_ke_band_loss": ([vp, vp, i32, i32, C.POINTER(dbl), vp, vp], C.c_int),
+            "gmt_adjoint_step": ([vp, vp, vp, vp, A, vp], C.c_int),
+            "gmt_adjoint_amp_grad": ([vp, C.POINTER(dbl), i32, vp], C.c_int),
             "gmt_run": ([vp, vp, vp, i32, dbl, dbl, i32, vp, C.POINTER(dbl), C.POINTER(i32)], C.c_int),
             "gmt_ensemble_create": ([P, i32, C.POINTER(i32), C.POINTER(dbl), C.POINTER(C.c_uint32), C.POINTER(vp)],
                                     C.c_int),

@@ -1,0 +1,425 @@
+// gmt_adjoint.cuh -- per-cell passes of the discrete adjoint of the unsplit GLM step (PLM-MC /
+// minmod, any Riemann solver, GLM, void floor, psi damping, forcing kick) with dt frozen.
+//
+// Given the step's input state u and the adjoint ubar' = dL/du' of its output, the passes form
+// ubar = (du'/du)^T ubar' and dL/d(forcing amplitude) of the step (periodic wrap):
+//   1 faces    forward reconstruction of every cell -> its 6 interface states FS
+//   2 fluxes   forward Riemann solve at every cell's +x,+y,+z face -> FL
+//   3 update   r1 = u + dt/dx * sum(F_lo - F_hi); adjoint of the epilogue (floor, psi damping,
+//              forcing kick) -> R1bar; ubar = R1bar (identity part); kick amplitude partials
+//   4 riemann  Fbar = dt/dx (R1bar[c+d] - R1bar[c]) -> adjoint interface states FSbar
+//   5 recon    faces -> (mh, m0, slopes) bars; the Hancock block mh = c2p(p2c(m0) - dt/2dx sum_d
+//              [F_d(m0+s_d) - F_d(m0-s_d)]) by one vector-Jacobian product per flux; limiter
+//              derivatives split each slope bar onto the three cells of its stencil
+//   6 gather   qbar(c) = own + neighbours' slope terms; ubar += (dq/du)^T qbar
+// The Riemann solvers, the directional fluxes, the epilogue, prim2cons and cons2prim are
+// differentiated by running the forward physics functions on forward-mode duals seeded in chunks
+// (the seeds are selects on a chunk offset, so no tangent is ever indexed dynamically); each
+// vector-Jacobian product is exact for the code that ran forward.  The limiter derivative, the
+// face/revert structure, the Hancock sum and the flux-difference identity are written out.  At a
+// limiter kink, an HLLD fan switch, a floor or an interface-state revert the derivative of the
+// branch that was taken is used (a subgradient).
+//
+// Every pass is a host-device function of one cell, so the same code also runs on the host.
+#pragma once
+#include "gmt_dual.cuh"
+#include "gmt_internal.h"
+
+namespace gmt {
+
+
+constexpr int NCH = 3;   // tangents per dual pass
+
+// xbar = (df/dx)^T ybar for f: 9 -> 9, by forward-mode passes of NC tangents each
+template <int NC, class R, class Fn> GMT_HD Q9<R> vjp9(Fn f, const Q9<R>& x, const Q9<R>& yb) {
+    using DD = Dual<R, NC>;
+    Q9<R> xb;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) xb.v[v] = R(0);
+#pragma unroll 1
+    for (int c0 = 0; c0 < 9; c0 += NC) {
+        Q9<DD> xd;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            xd.v[v] = DD(x.v[v]);
+#pragma unroll
+            for (int j = 0; j < NC; ++j) xd.v[v].d[j] = (c0 + j == v) ? R(1) : R(0);
+        }
+        Q9<DD> y = f(xd);
+#pragma unroll
+        for (int j = 0; j < NC; ++j) {
+            R acc = R(0);
+#pragma unroll
+            for (int v = 0; v < 9; ++v) acc += yb.v[v] * y.v[v].d[j];
+#pragma unroll
+            for (int v = 0; v < 9; ++v)
+                if (c0 + j == v) xb.v[v] = acc;
+        }
+    }
+    return xb;
+}
+
+template <class R> GMT_HD void q9_add(Q9<R>& a, const Q9<R>& b, R s = R(1)) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) a.v[v] += s * b.v[v];
+}
+template <class R> GMT_HD Q9<R> q9_zero() {
+    Q9<R> a;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) a.v[v] = R(0);
+    return a;
+}
+
+template <class R> struct Idx {
+    int nx, ny, nz;
+    size_t n;
+    GMT_HD size_t at(int x, int y, int z) const {
+        return (size_t)wrapi(x, nx) + (size_t)nx * ((size_t)wrapi(y, ny) + (size_t)ny * wrapi(z, nz));
+    }
+};
+
+template <class R> GMT_HD Q9<R> load_u(const CPlanes<R>& u, size_t c) {
+    Q9<R> q;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) q.v[v] = u.p[v][c];
+    return q;
+}
+
+// the six interface states of one cell (recon_prims + face_state of the forward kernel)
+template <class R> struct CellRec {
+    Q9<R> m0, uh, mh, s[3], L[3], Rr[3];
+    bool hrev;        // the predictor reverted to m0
+    bool bad[6];      // the face state reverted to m0
+};
+
+template <class R>
+GMT_HD void cell_rec(const CPlanes<R>& u, const Idx<R>& I, int x, int y, int z, const Consts<R>& K,
+                                         R dtdx, int iflo, bool mm, CellRec<R>& r) {
+    r.m0 = cons2prim(load_u(u, I.at(x, y, z)), K.gamma, K.smallr, K.pfl);
+    r.L[0] = cons2prim(load_u(u, I.at(x - 1, y, z)), K.gamma, K.smallr, K.pfl);
+    r.Rr[0] = cons2prim(load_u(u, I.at(x + 1, y, z)), K.gamma, K.smallr, K.pfl);
+    r.L[1] = cons2prim(load_u(u, I.at(x, y - 1, z)), K.gamma, K.smallr, K.pfl);
+    r.Rr[1] = cons2prim(load_u(u, I.at(x, y + 1, z)), K.gamma, K.smallr, K.pfl);
+    r.L[2] = cons2prim(load_u(u, I.at(x, y, z - 1)), K.gamma, K.smallr, K.pfl);
+    r.Rr[2] = cons2prim(load_u(u, I.at(x, y, z + 1)), K.gamma, K.smallr, K.pfl);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            R dl = r.m0.v[v] - r.L[d].v[v], dr = r.Rr[d].v[v] - r.m0.v[v];
+            r.s[d].v[v] = mm ? R(0.5) * minmod(dl, dr) : R(0.5) * moncen(dl, dr);
+        }
+    r.uh = hancock(r.m0, r.s[0], r.s[1], r.s[2], dtdx, K.gamma);
+    r.mh = cons2prim(r.uh, K.gamma, K.smallr, K.pfl);
+    r.hrev = r.mh.v[0] <= K.smallr || r.mh.v[4] <= K.pfl;
+    if (r.hrev) r.mh = r.m0;
+}
+
+template <class R>
+GMT_HD Q9<R> rec_face(const CellRec<R>& r, int k, const Consts<R>& K, int iflo, bool& bad) {
+    const int d = k >> 1;
+    Q9<R> f = padd(r.mh, r.s[d], (k & 1) ? R(-1) : R(1));
+    bad = iflo && (f.v[0] < K.smallr || f.v[4] < K.pfl);
+    return bad ? r.m0 : f;
+}
+
+// derivatives of the half slope g(dl, dr) (MonCen or minmod) w.r.t. dl and dr
+template <class R> GMT_HD void slope_deriv(R dl, R dr, bool mm, R& gl, R& gr) {
+    gl = R(0);
+    gr = R(0);
+    if (dl * dr <= R(0)) return;
+    if (mm) {
+        if (rabs(dl) < rabs(dr)) gl = R(0.5); else gr = R(0.5);
+        return;
+    }
+    R dc = R(0.5) * (dl + dr);
+    R m2 = R(2) * rmin(rabs(dl), rabs(dr));
+    if (m2 <= rabs(dc)) {                          // rmin(m2, |dc|) picks m2
+        if (rabs(dl) <= rabs(dr)) gl = R(1); else gr = R(1);
+    } else {
+        gl = R(0.25);
+        gr = R(0.25);
+    }
+}
+
+template <int D, class R>
+GMT_HD Q9<R> riemann_any(const Q9<R>& L, const Q9<R>& Rr, const Consts<R>& K, R ch, bool use_llf,
+                                             int riem) {
+    if (riem == RIEM_HLL) return riemann_glm<D, RIEM_HLL>(L, Rr, K, ch, use_llf);
+    if (riem == RIEM_LLF_BOUND) return riemann_glm<D, RIEM_LLF_BOUND>(L, Rr, K, ch, use_llf);
+    return riemann_glm<D, RIEM_HLLD>(L, Rr, K, ch, use_llf);
+}
+
+// Lbar, Rbar = J^T Fbar of the Riemann solve at a D face (18 inputs in chunks of NCH)
+template <int D, class R>
+GMT_HD void riemann_adj(const Q9<R>& L, const Q9<R>& Rr, const Q9<R>& Fb, const Consts<R>& K, R ch,
+                                            bool use_llf, int riem, Q9<R>& Lb, Q9<R>& Rb) {
+    using DD = Dual<R, NCH>;
+    const Consts<DD> KD = dual_consts<R, NCH>(K);
+    Lb = q9_zero<R>();
+    Rb = q9_zero<R>();
+#pragma unroll 1
+    for (int c0 = 0; c0 < 18; c0 += NCH) {
+        Q9<DD> Ld, Rd;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            Ld.v[v] = DD(L.v[v]);
+            Rd.v[v] = DD(Rr.v[v]);
+#pragma unroll
+            for (int j = 0; j < NCH; ++j) {
+                Ld.v[v].d[j] = (c0 + j == v) ? R(1) : R(0);
+                Rd.v[v].d[j] = (c0 + j == 9 + v) ? R(1) : R(0);
+            }
+        }
+        Q9<DD> F = riemann_any<D>(Ld, Rd, KD, DD(ch), use_llf, riem);
+#pragma unroll
+        for (int j = 0; j < NCH; ++j) {
+            R acc = R(0);
+#pragma unroll
+            for (int v = 0; v < 9; ++v) acc += Fb.v[v] * F.v[v].d[j];
+#pragma unroll
+            for (int v = 0; v < 9; ++v) {
+                if (c0 + j == v) Lb.v[v] = acc;
+                if (c0 + j == 9 + v) Rb.v[v] = acc;
+            }
+        }
+    }
+}
+
+
+template <class R> GMT_HD void cell_xyz(const AdjArgs<R>& A, size_t c, int& x, int& y, int& z) {
+    x = (int)(c % A.nx);
+    y = (int)((c / A.nx) % A.ny);
+    z = (int)(c / ((size_t)A.nx * A.ny));
+}
+template <class R> GMT_HD Idx<R> idx_of(const AdjArgs<R>& A) {
+    return Idx<R>{A.nx, A.ny, A.nz, (size_t)A.nx * A.ny * A.nz};
+}
+template <class R> GMT_HD Q9<R> fs_get(const R* FS, size_t n, size_t c, int k) {
+    Q9<R> q;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) q.v[v] = FS[(size_t)(k * 9 + v) * n + c];
+    return q;
+}
+
+template <class R> struct FluxFn {
+    R gamma;
+    int d;
+    template <class T> GMT_HD Q9<T> operator()(const Q9<T>& q) const {
+        if (d == 0) return dir_flux<0>(q, T(gamma));
+        if (d == 1) return dir_flux<1>(q, T(gamma));
+        return dir_flux<2>(q, T(gamma));
+    }
+};
+template <class R> struct C2PFn {
+    Consts<R> K;
+    template <class T> GMT_HD Q9<T> operator()(const Q9<T>& q) const {
+        return cons2prim(q, T(K.gamma), T(K.smallr), T(K.pfl));
+    }
+};
+template <class R> struct P2CFn {
+    R gamma;
+    template <class T> GMT_HD Q9<T> operator()(const Q9<T>& q) const { return prim2cons(q, T(gamma)); }
+};
+
+// pass 1: the six interface states of cell c
+template <class R> GMT_HD void adj_faces_cell(const AdjArgs<R>& A, size_t c) {
+    const Idx<R> I = idx_of(A);
+    int x, y, z;
+    cell_xyz(A, c, x, y, z);
+    CellRec<R> r;
+    cell_rec(A.u, I, x, y, z, A.K, A.dtdx, A.iflo, A.recon == RECON_MINMOD, r);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        bool bad;
+        Q9<R> f = rec_face(r, k, A.K, A.iflo, bad);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) A.FS[(size_t)(k * 9 + v) * I.n + c] = f.v[v];
+    }
+}
+
+// pass 2: the fluxes at the +x, +y, +z faces of cell c
+template <class R> GMT_HD void adj_flux_cell(const AdjArgs<R>& A, size_t c) {
+    const Idx<R> I = idx_of(A);
+    const bool ul = A.use_llf != 0;
+    int x, y, z;
+    cell_xyz(A, c, x, y, z);
+    Q9<R> F0 = riemann_any<0>(fs_get(A.FS, I.n, c, 0), fs_get(A.FS, I.n, I.at(x + 1, y, z), 1), A.K, A.ch, ul, A.riem);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) A.FL[(size_t)v * I.n + c] = F0.v[v];
+    Q9<R> F1 = riemann_any<1>(fs_get(A.FS, I.n, c, 2), fs_get(A.FS, I.n, I.at(x, y + 1, z), 3), A.K, A.ch, ul, A.riem);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) A.FL[(size_t)(9 + v) * I.n + c] = F1.v[v];
+    Q9<R> F2 = riemann_any<2>(fs_get(A.FS, I.n, c, 4), fs_get(A.FS, I.n, I.at(x, y, z + 1), 5), A.K, A.ch, ul, A.riem);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) A.FL[(size_t)(18 + v) * I.n + c] = F2.v[v];
+}
+
+// pass 3: the update and its epilogue; returns this cell's part of dL/d(amplitude)
+template <class R> GMT_HD double adj_update_cell(const AdjArgs<R>& A, size_t c) {
+    constexpr int NU = 6;
+    using DD = Dual<R, NU>;
+    const Idx<R> I = idx_of(A);
+    const bool turb = A.do_turb && A.btab != nullptr;
+    const Consts<DD> KD = dual_consts<R, NU>(A.K);
+    int x, y, z;
+    cell_xyz(A, c, x, y, z);
+    const size_t cxm = I.at(x - 1, y, z), cym = I.at(x, y - 1, z), czm = I.at(x, y, z - 1);
+    Q9<R> r1;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+        R fxl = A.FL[(size_t)v * I.n + cxm], fxh = A.FL[(size_t)v * I.n + c];
+        R fyl = A.FL[(size_t)(9 + v) * I.n + cym], fyh = A.FL[(size_t)(9 + v) * I.n + c];
+        R fzl = A.FL[(size_t)(18 + v) * I.n + czm], fzh = A.FL[(size_t)(18 + v) * I.n + c];
+        r1.v[v] = A.u.p[v][c] + A.dtdx * (((fxl - fxh) + (fyl - fyh)) + (fzl - fzh));
+    }
+    R a3[3] = {R(0), R(0), R(0)};
+    if (turb) force_accel(A.btab + ((size_t)z * A.ny + y) * 24, A.trigx, A.nx, x, A.ramp, a3[0], a3[1], a3[2]);
+    const Q9<R> ob = load_u(A.ubn, c);
+    Q9<R> rb;
+    R abar[3] = {R(0), R(0), R(0)};
+#pragma unroll
+    for (int c0 = 0; c0 < 12; c0 += NU) {   // two passes: the 9 state inputs, then the 3 accelerations
+        Q9<DD> q;
+        DD ad[3];
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            q.v[v] = DD(r1.v[v]);
+#pragma unroll
+            for (int j = 0; j < NU; ++j) q.v[v].d[j] = (c0 + j == v) ? R(1) : R(0);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            ad[i] = DD(a3[i]);
+#pragma unroll
+            for (int j = 0; j < NU; ++j) ad[i].d[j] = (c0 + j == 9 + i) ? R(1) : R(0);
+        }
+        finish_update(q, KD, DD(A.glm_fac), turb, ad[0], ad[1], ad[2], DD(A.dt));
+#pragma unroll
+        for (int j = 0; j < NU; ++j) {
+            R acc = R(0);
+#pragma unroll
+            for (int v = 0; v < 9; ++v) acc += ob.v[v] * q.v[v].d[j];
+            const int i = c0 + j;
+            if (i < 9) rb.v[i] = acc;
+            else if (i < 12) abar[i - 9] = acc;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+        A.R1b[(size_t)v * I.n + c] = rb.v[v];
+        A.ub.p[v][c] = rb.v[v];
+    }
+    if (turb && A.amp != R(0))
+        return ((double)abar[0] * a3[0] + (double)abar[1] * a3[1] + (double)abar[2] * a3[2]) / (double)A.amp;
+    return 0.0;
+}
+
+// pass 4: adjoint of the Riemann solves at the +x, +y, +z faces of cell c
+template <class R> GMT_HD void adj_riemann_cell(const AdjArgs<R>& A, size_t c) {
+    const Idx<R> I = idx_of(A);
+    const bool ul = A.use_llf != 0;
+    int x, y, z;
+    cell_xyz(A, c, x, y, z);
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+        const size_t cp = d == 0 ? I.at(x + 1, y, z) : (d == 1 ? I.at(x, y + 1, z) : I.at(x, y, z + 1));
+        Q9<R> Fb, Lb, Rb;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) Fb.v[v] = A.dtdx * (A.R1b[(size_t)v * I.n + cp] - A.R1b[(size_t)v * I.n + c]);
+        const Q9<R> L = fs_get(A.FS, I.n, c, 2 * d), Rr = fs_get(A.FS, I.n, cp, 2 * d + 1);
+        if (d == 0) riemann_adj<0>(L, Rr, Fb, A.K, A.ch, ul, A.riem, Lb, Rb);
+        else if (d == 1) riemann_adj<1>(L, Rr, Fb, A.K, A.ch, ul, A.riem, Lb, Rb);
+        else riemann_adj<2>(L, Rr, Fb, A.K, A.ch, ul, A.riem, Lb, Rb);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            A.FSb[(size_t)((2 * d) * 9 + v) * I.n + c] = Lb.v[v];
+            A.FSb[(size_t)((2 * d + 1) * 9 + v) * I.n + cp] = Rb.v[v];
+        }
+    }
+}
+
+// pass 5: adjoint of the reconstruction of cell c
+template <class R> GMT_HD void adj_recon_cell(const AdjArgs<R>& A, size_t c) {
+    const Idx<R> I = idx_of(A);
+    const bool mm = A.recon == RECON_MINMOD;
+    int x, y, z;
+    cell_xyz(A, c, x, y, z);
+    CellRec<R> r;
+    cell_rec(A.u, I, x, y, z, A.K, A.dtdx, A.iflo, mm, r);
+    // faces: f = mh +- s_d, or m0 where reverted
+    Q9<R> m0b = q9_zero<R>(), mhb = q9_zero<R>(), sb[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sb[d] = q9_zero<R>();
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        bool bad;
+        (void)rec_face(r, k, A.K, A.iflo, bad);
+        const Q9<R> fb = fs_get(A.FSb, I.n, c, k);
+        if (bad) {
+            q9_add(m0b, fb);
+        } else {
+            q9_add(mhb, fb);
+            q9_add(sb[k >> 1], fb, (k & 1) ? R(-1) : R(1));
+        }
+    }
+    // predictor: mh = c2p(p2c(m0) - h sum_d [F_d(m0 + s_d) - F_d(m0 - s_d)]), or m0 if reverted
+    if (r.hrev) {
+        q9_add(m0b, mhb);
+    } else {
+        const Q9<R> uhb = vjp9<3>(C2PFn<R>{A.K}, r.uh, mhb);
+        q9_add(m0b, vjp9<3>(P2CFn<R>{A.K.gamma}, r.m0, uhb));
+        Q9<R> Fb;
+        const R h = R(0.5) * A.dtdx;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) Fb.v[v] = -h * uhb.v[v];
+#pragma unroll 1
+        for (int d = 0; d < 3; ++d) {
+            const Q9<R> jp = vjp9<3>(FluxFn<R>{A.K.gamma, d}, padd(r.m0, r.s[d], R(1)), Fb);
+            const Q9<R> jm = vjp9<3>(FluxFn<R>{A.K.gamma, d}, padd(r.m0, r.s[d], R(-1)), Fb);
+#pragma unroll
+            for (int v = 0; v < 9; ++v) {
+                m0b.v[v] += jp.v[v] - jm.v[v];
+                sb[d].v[v] += jp.v[v] + jm.v[v];
+            }
+        }
+    }
+    // limiter: s_d = g(m0 - L_d, R_d - m0); m0 gets (gl - gr) sbar, the neighbours -gl sbar, +gr sbar
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+        R own = m0b.v[v];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            R gl, gr;
+            slope_deriv(r.m0.v[v] - r.L[d].v[v], r.Rr[d].v[v] - r.m0.v[v], mm, gl, gr);
+            const R Ad = sb[d].v[v] * gl, Bd = sb[d].v[v] * gr;
+            own += Ad - Bd;
+            A.QB[(size_t)(9 + 9 * d + v) * I.n + c] = Ad;
+            A.QB[(size_t)(36 + 9 * d + v) * I.n + c] = Bd;
+        }
+        A.QB[(size_t)v * I.n + c] = own;
+    }
+}
+
+// pass 6: gather the primitive adjoint of cell c and map it through cons2prim
+template <class R> GMT_HD void adj_gather_cell(const AdjArgs<R>& A, size_t c) {
+    const Idx<R> I = idx_of(A);
+    int x, y, z;
+    cell_xyz(A, c, x, y, z);
+    const size_t cp[3] = {I.at(x + 1, y, z), I.at(x, y + 1, z), I.at(x, y, z + 1)};
+    const size_t cm[3] = {I.at(x - 1, y, z), I.at(x, y - 1, z), I.at(x, y, z - 1)};
+    Q9<R> qb;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+        R s = A.QB[(size_t)v * I.n + c];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            s += -A.QB[(size_t)(9 + 9 * d + v) * I.n + cp[d]] + A.QB[(size_t)(36 + 9 * d + v) * I.n + cm[d]];
+        qb.v[v] = s;
+    }
+    const Q9<R> ubq = vjp9<3>(C2PFn<R>{A.K}, load_u(A.u, c), qb);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) A.ub.p[v][c] += ubq.v[v];
+}
+
+}  // namespace gmt

@@ -90,6 +90,8 @@ struct gmt_ctx {
     size_t spec_bytes = 0;
     uint32_t counter = 0;
     double sigma0 = 0, alpha = 0, beta = 0;
+    void* adj = nullptr;           // adjoint scratch (207 planes, allocated on first use)
+    double* adj_damp = nullptr;    // dL/d(turb_amp) accumulator
 };
 
 namespace {
@@ -385,6 +387,8 @@ int gmt_destroy(gmt_ctx* c) {
     cudaFree(c->err);
     for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
     cudaFree(c->spec);
+    cudaFree(c->adj);
+    cudaFree(c->adj_damp);
     if (c->cap) cudaStreamDestroy(c->cap);
     cudaFree(c->loop);
     cudaFree(c->loopc);
@@ -515,6 +519,86 @@ int gmt_ke_spectrum(gmt_ctx* c, const void* u, int32_t kmax, double* out, void* 
                         ? launch_spectrum<double>(cplanes<double>(u, c->n), c->p.nx, c->p.ny, c->p.nz, kmax, c->spec, out, s)
                         : launch_spectrum<float>(cplanes<float>(u, c->n), c->p.nx, c->p.ny, c->p.nz, kmax, c->spec, out, s);
     return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_ke_spectrum");
+}
+
+int gmt_ke_band_loss(gmt_ctx* c, const void* u, int32_t kmin, int32_t kmax, double* loss, void* ubar, void* stream) {
+    if (!c || !u || !loss) return fail(GMT_ERR_ARG, "gmt_ke_band_loss: null argument");
+    if (c->p.scheme == GMT_SCHEME_CT) return fail(GMT_ERR_ARG, "gmt_ke_band_loss: GLM state only");
+    if (kmin < 0 || kmax < kmin || kmax < 1 || 2 * kmax + 1 > std::min(c->p.ny, c->p.nz) || kmax + 1 > c->p.nx)
+        return fail(GMT_ERR_ARG, "gmt_ke_band_loss: need 0 <= kmin <= kmax, 1 <= kmax, 2*kmax+1 <= grid size");
+    size_t need = band_scratch_bytes(c->p.nx, c->p.ny, c->p.nz, kmax);
+    if (need > c->spec_bytes) {
+        cudaFree(c->spec);
+        c->spec = nullptr;
+        c->spec_bytes = 0;
+        GMT_CUDA(cudaMalloc(&c->spec, need));
+        c->spec_bytes = need;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!ubar) return fail(GMT_ERR_ARG, "gmt_ke_band_loss: ubar is required (9 planes of the state's dtype)");
+    void* ub = ubar;
+    cudaError_t e = c->esize == 8
+        ? launch_band_loss<double>(cplanes<double>(u, c->n), c->p.nx, c->p.ny, c->p.nz, kmin, kmax, c->spec, loss,
+                                   planes<double>(ub, c->n), s)
+        : launch_band_loss<float>(cplanes<float>(u, c->n), c->p.nx, c->p.ny, c->p.nz, kmin, kmax, c->spec, loss,
+                                  planes<float>(ub, c->n), s);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_ke_band_loss");
+}
+
+int gmt_adjoint_step(gmt_ctx* c, const void* u, const void* ubar_next, void* ubar, const gmt_step_args* a,
+                     void* stream) {
+    if (!c || !u || !ubar_next || !ubar || !a) return fail(GMT_ERR_ARG, "gmt_adjoint_step: null argument");
+    const gmt_params& p = c->p;
+    if (p.scheme != GMT_SCHEME_UNSPLIT) return fail(GMT_ERR_ARG, "gmt_adjoint_step: unsplit GLM contexts only");
+    if (p.recon == GMT_RECON_PPM) return fail(GMT_ERR_ARG, "gmt_adjoint_step: PLM (MC or minmod) only");
+    if (ubar == u || ubar == ubar_next) return fail(GMT_ERR_ARG, "gmt_adjoint_step: ubar aliases an input");
+    if (!(a->dt > 0.0) || !std::isfinite(a->dt)) return fail(GMT_ERR_ARG, "dt must be positive and finite");
+    if (!(a->ch > 0.0)) return fail(GMT_ERR_ARG, "ch must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!c->adj) {
+        GMT_CUDA(cudaMalloc(&c->adj, adjoint_scratch_reals(c->n) * c->esize));
+        GMT_CUDA(cudaMalloc(&c->adj_damp, sizeof(double)));
+        GMT_CUDA(cudaMemsetAsync(c->adj_damp, 0, sizeof(double), s));
+    }
+    const double dx = p.boxlen / p.nx;
+    auto go = [&](auto zero) -> int {
+        using R = decltype(zero);
+        AdjArgs<R> A;
+        A.u = cplanes<R>(u, c->n);
+        A.ubn = cplanes<R>(ubar_next, c->n);
+        A.ub = planes<R>(ubar, c->n);
+        A.nx = p.nx; A.ny = p.ny; A.nz = p.nz;
+        A.dt = (R)a->dt; A.dtdx = A.dt / (R)dx;
+        A.ch = (R)a->ch; A.glm_fac = (R)a->glm_fac;
+        A.ramp = (R)(p.turb_T > 0 ? std::min(a->t / p.turb_T, 1.0) : 1.0);
+        A.amp = (R)p.turb_amp;
+        A.K = consts_of<R>(p);
+        A.iflo = p.iflo; A.use_llf = p.riemann == GMT_RIEMANN_LLF; A.do_turb = a->do_turb;
+        A.recon = p.recon;
+        A.riem = p.riemann == GMT_RIEMANN_LLF ? GMT_RIEMANN_HLLD : p.riemann;
+        A.btab = a->do_turb ? static_cast<const R*>(c->btab) : nullptr;
+        A.trigx = static_cast<const R*>(c->trig[0]);
+        R* base = static_cast<R*>(c->adj);
+        A.FS = base;
+        A.FL = A.FS + 54 * c->n;
+        A.R1b = A.FL + 27 * c->n;
+        A.FSb = A.R1b + 9 * c->n;
+        A.QB = A.FSb + 54 * c->n;
+        A.damp = c->adj_damp;
+        cudaError_t e = launch_adjoint<R>(A, s);
+        return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_adjoint_step");
+    };
+    return c->esize == 8 ? go(0.0) : go(0.0f);
+}
+
+int gmt_adjoint_amp_grad(gmt_ctx* c, double* out, int32_t reset, void* stream) {
+    if (!c || !out) return fail(GMT_ERR_ARG, "gmt_adjoint_amp_grad: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!c->adj_damp) { *out = 0.0; return GMT_OK; }
+    GMT_CUDA(cudaMemcpyAsync(out, c->adj_damp, sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (reset) GMT_CUDA(cudaMemsetAsync(c->adj_damp, 0, sizeof(double), s));
+    GMT_CUDA(cudaStreamSynchronize(s));
+    return GMT_OK;
 }
 
 int gmt_forcing_reset(gmt_ctx* c, void* stream) {

@@ -101,7 +101,7 @@ template <class R> __device__ __forceinline__ void cp_async_r(R* smem, const R* 
 template <> __device__ __forceinline__ void cp_async_r(float* s, const float* g) { cp_async4(s, g); }
 template <> __device__ __forceinline__ void cp_async_r(double* s, const double* g) { cp_async8(s, g); }
 
-__device__ __forceinline__ int wrapi(int i, int n) {
+GMT_HD int wrapi(int i, int n) {
     i = i % n;
     return i < 0 ? i + n : i;
 }
@@ -210,7 +210,7 @@ __device__ __forceinline__ void btab_row(const double* modes, const int* mode_k,
 
 // forcing acceleration at one cell from the per-row table (same order as the oracle)
 template <class R>
-__device__ __forceinline__ void force_accel(const R* btab_row, const R* trigx, int nx, int i, R ramp, R& ax, R& ay,
+GMT_HD void force_accel(const R* btab_row, const R* trigx, int nx, int i, R ramp, R& ax, R& ay,
                                             R& az) {
     R S0 = R(0), S1 = R(0), S2 = R(0);
 #pragma unroll

@@ -78,6 +78,29 @@ template <class R> cudaError_t launch_ic_turb(const Planes<R>& u, int nx, int ny
 size_t spectrum_scratch_bytes(int nx, int ny, int nz, int kmax);
 template <class R> cudaError_t launch_spectrum(const CPlanes<R>& u, int nx, int ny, int nz, int kmax, void* scratch,
                                                double* E_host, cudaStream_t s);
+size_t band_scratch_bytes(int nx, int ny, int nz, int kmax);
+template <class R> cudaError_t launch_band_loss(const CPlanes<R>& u, int nx, int ny, int nz, int kmin, int kmax,
+                                                void* scratch, double* L_host, const Planes<R>& ub, cudaStream_t s);
+// discrete adjoint of one unsplit PLM step, dt frozen (gmt_adjoint.cu)
+template <class R> struct AdjArgs {
+    CPlanes<R> u;          // input state of the forward step
+    CPlanes<R> ubn;        // adjoint of the step's output
+    Planes<R> ub;          // adjoint of the step's input (written)
+    int nx, ny, nz;
+    R dt, dtdx, ch, glm_fac, ramp, amp;
+    Consts<R> K;
+    int iflo, use_llf, do_turb, recon, riem;
+    const R* btab;
+    const R* trigx;
+    R* FS;                 // 54 planes: the 6 interface states of every cell
+    R* FL;                 // 27 planes: the +x, +y, +z face fluxes
+    R* R1b;                // 9 planes: adjoint of the pre-epilogue update
+    R* FSb;                // 54 planes: adjoint of the interface states
+    R* QB;                 // 63 planes: own primitive adjoint (9), slope-stencil terms A_d (27), B_d (27)
+    double* damp;          // dL/d(forcing amplitude) accumulator
+};
+size_t adjoint_scratch_reals(size_t n);
+template <class R> cudaError_t launch_adjoint(const AdjArgs<R>& A, cudaStream_t s);
 cudaError_t upload_mode_table();   // the 61 wavevectors into constant memory
 cudaError_t mode_table_device(const int** ptr);   // device address of that table
 void set_last_error(const std::string& msg);   // message returned by gmt_last_error() on this thread

@@ -12,7 +12,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#define GMT_HD __device__ __forceinline__
+#define GMT_HD __host__ __device__ __forceinline__
 
 namespace gmt {
 

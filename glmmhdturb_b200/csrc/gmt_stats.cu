@@ -147,6 +147,167 @@ cudaError_t launch_spectrum(const CPlanes<R>& u, int nx, int ny, int nz, int kma
     return e;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Band-limited kinetic-energy loss L = sum_{kmin <= shell <= kmax} E(shell) and its gradient.
+// dL/dw(x) = w_S(x)/N^3 with w_S the band-passed field, pulled back through w = m/sqrt(rho).
+// ---------------------------------------------------------------------------------------------
+// stage z of the forward transform, complex: C[c][kx][jy][jz] = N^-3 sum_z B e^{-i kz z}
+__global__ void __launch_bounds__(128) band_z_kernel(const double2* B, int nz, int kmax, const double2* tw, double norm,
+                                                     double2* Cc) {
+    const int K1 = kmax + 1, K2 = 2 * kmax + 1;
+    const size_t total = 3 * (size_t)K1 * K2 * K2;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int jz = (int)(t % K2);
+        const size_t ckxjy = t / K2;
+        const double2* b = B + ckxjy * nz;
+        const double2* e = tw + (size_t)jz * nz;
+        double re = 0.0, im = 0.0;
+        for (int z = 0; z < nz; ++z) {
+            re += b[z].x * e[z].x - b[z].y * e[z].y;
+            im += b[z].x * e[z].y + b[z].y * e[z].x;
+        }
+        Cc[t] = make_double2(re * norm, im * norm);
+    }
+}
+
+__device__ __forceinline__ int shell_of(int kx, int ky, int kz) {
+    return (int)floor(sqrt((double)(kx * kx + ky * ky + kz * kz)) + 0.5);
+}
+
+// loss, one thread, fixed order
+__global__ void band_loss_kernel(const double2* Cc, int kmax, int kmin, int kmaxb, double* L) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int K1 = kmax + 1, K2 = 2 * kmax + 1;
+    double acc = 0.0;
+    for (int c = 0; c < 3; ++c)
+        for (int kx = 0; kx < K1; ++kx)
+            for (int jy = 0; jy < K2; ++jy)
+                for (int jz = 0; jz < K2; ++jz) {
+                    int sh = shell_of(kx, jy - kmax, jz - kmax);
+                    if (sh < kmin || sh > kmaxb) continue;
+                    double2 v = Cc[(((size_t)c * K1 + kx) * K2 + jy) * K2 + jz];
+                    acc += 0.5 * (kx > 0 ? 2.0 : 1.0) * (v.x * v.x + v.y * v.y);
+                }
+    *L = acc;
+}
+
+// inverse z: G[c][kx][jy][z] = sum_jz mask * C e^{+i kz z}   (tw holds e^{-i k z}: use its conjugate)
+__global__ void __launch_bounds__(128) band_iz_kernel(const double2* Cc, int nz, int kmax, int kmin, int kmaxb,
+                                                      const double2* tw, double2* G) {
+    const int K1 = kmax + 1, K2 = 2 * kmax + 1;
+    const size_t total = 3 * (size_t)K1 * K2 * nz;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int z = (int)(t % nz);
+        const size_t ckxjy = t / nz;
+        const int jy = (int)(ckxjy % K2), kx = (int)((ckxjy / K2) % K1);
+        double re = 0.0, im = 0.0;
+        for (int jz = 0; jz < K2; ++jz) {
+            int sh = shell_of(kx, jy - kmax, jz - kmax);
+            if (sh < kmin || sh > kmaxb) continue;
+            double2 cv = Cc[ckxjy * K2 + jz];
+            double2 e = tw[(size_t)jz * nz + z];   // e^{-i kz z}; conj = e^{+i kz z}
+            re += cv.x * e.x + cv.y * e.y;
+            im += cv.y * e.x - cv.x * e.y;
+        }
+        G[t] = make_double2(re, im);
+    }
+}
+
+// inverse y: H[c][kx][y + ny z] = sum_jy G[c][kx][jy][z] e^{+i ky y}
+__global__ void __launch_bounds__(128) band_iy_kernel(const double2* G, int ny, int nz, int kmax, const double2* tw,
+                                                      double2* H) {
+    const int K1 = kmax + 1, K2 = 2 * kmax + 1;
+    const size_t rows = (size_t)ny * nz;
+    const size_t total = 3 * (size_t)K1 * rows;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t row = t % rows;
+        const size_t ckx = t / rows;
+        const int y = (int)(row % ny), z = (int)(row / ny);
+        double re = 0.0, im = 0.0;
+        for (int jy = 0; jy < K2; ++jy) {
+            double2 g = G[(ckx * K2 + jy) * nz + z];
+            double2 e = tw[(size_t)jy * ny + y];
+            re += g.x * e.x + g.y * e.y;
+            im += g.y * e.x - g.x * e.y;
+        }
+        H[t] = make_double2(re, im);
+    }
+}
+
+// inverse x + chain rule: wS_c = sum_kx wgt Re(H e^{+i kx x}); ubar = dL/du
+template <class R>
+__global__ void __launch_bounds__(128) band_ix_kernel(const CPlanes<R> u, int nx, int ny, int nz, int kmax,
+                                                      const double2* H, const double2* tw, double norm, Planes<R> ub) {
+    const size_t rows = (size_t)ny * nz;
+    const size_t n = rows * nx;
+    const int K1 = kmax + 1;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(c % nx);
+        const size_t row = c / nx;
+        double rho = fmax((double)u.p[0][c], 1e-300), isr = 1.0 / sqrt(rho);
+        double rhob = 0.0;
+        for (int comp = 0; comp < 3; ++comp) {
+            double ws = 0.0;
+            for (int kx = 0; kx < K1; ++kx) {
+                double2 h = H[((size_t)comp * K1 + kx) * rows + row];
+                double2 e = tw[(size_t)kx * nx + x];
+                ws += (kx > 0 ? 2.0 : 1.0) * (h.x * e.x + h.y * e.y);   // Re(h * conj(e))
+            }
+            double wb = ws * norm;
+            double m = (double)u.p[1 + comp][c];
+            ub.p[1 + comp][c] = (R)(wb * isr);
+            rhob += -0.5 * wb * m * isr / rho;
+        }
+        ub.p[0][c] = (R)rhob;
+        for (int v = 4; v < 9; ++v) ub.p[v][c] = (R)0;
+    }
+}
+
+template <class R>
+cudaError_t launch_band_loss(const CPlanes<R>& u, int nx, int ny, int nz, int kmin, int kmax, void* scratch, double* L_host,
+                             const Planes<R>& ub, cudaStream_t s) {
+    const size_t K1 = kmax + 1, K2 = 2 * kmax + 1;
+    char* p = static_cast<char*>(scratch);
+    double2* twx = reinterpret_cast<double2*>(p);
+    double2* twy = twx + K1 * nx;
+    double2* twz = twy + K2 * ny;
+    double2* A = twz + K2 * nz;
+    double2* B = A + 3 * K1 * (size_t)ny * nz;
+    double2* Cc = B + 3 * K1 * K2 * (size_t)nz;
+    double2* G = Cc + 3 * K1 * K2 * K2;
+    double* L = reinterpret_cast<double*>(G + 3 * K1 * K2 * (size_t)nz);
+    std::vector<double> tx = spectrum_twiddles(nx, 0, kmax), ty = spectrum_twiddles(ny, -kmax, kmax),
+                        tz = spectrum_twiddles(nz, -kmax, kmax);
+    cudaError_t e = cudaMemcpyAsync(twx, tx.data(), tx.size() * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(twy, ty.data(), ty.size() * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(twz, tz.data(), tz.size() * 8, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    const double n3 = (double)nx * ny * nz;
+    auto grid = [](size_t total) { return (int)std::min<size_t>((total + 127) / 128, 148 * 32); };
+    spec_x_kernel<R><<<grid(3 * K1 * ny * nz), 128, 0, s>>>(u, nx, ny, nz, kmax, twx, A);
+    spec_y_kernel<<<grid(3 * K1 * K2 * nz), 128, 0, s>>>(A, ny, nz, kmax, twy, B);
+    band_z_kernel<<<grid(3 * K1 * K2 * K2), 128, 0, s>>>(B, nz, kmax, twz, 1.0 / n3, Cc);
+    band_loss_kernel<<<1, 1, 0, s>>>(Cc, kmax, kmin, kmax, L);
+    band_iz_kernel<<<grid(3 * K1 * K2 * nz), 128, 0, s>>>(Cc, nz, kmax, kmin, kmax, twz, G);
+    band_iy_kernel<<<grid(3 * K1 * ny * nz), 128, 0, s>>>(G, ny, nz, kmax, twy, A);
+    band_ix_kernel<R><<<grid((size_t)nx * ny * nz), 128, 0, s>>>(u, nx, ny, nz, kmax, A, twx, 1.0 / n3, ub);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(L_host, L, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
+}
+
+size_t band_scratch_bytes(int nx, int ny, int nz, int kmax) {
+    const size_t K1 = kmax + 1, K2 = 2 * kmax + 1;
+    return 2 * sizeof(double) * (K1 * nx + K2 * ny + K2 * nz) + 3 * K1 * (size_t)ny * nz * sizeof(double2) +
+           3 * K1 * K2 * (size_t)nz * sizeof(double2) * 2 + 3 * K1 * K2 * K2 * sizeof(double2) + 256;
+}
+
+template cudaError_t launch_band_loss<float>(const CPlanes<float>&, int, int, int, int, int, void*, double*,
+                                             const Planes<float>&, cudaStream_t);
+template cudaError_t launch_band_loss<double>(const CPlanes<double>&, int, int, int, int, int, void*, double*,
+                                              const Planes<double>&, cudaStream_t);
+
 template cudaError_t launch_spectrum<float>(const CPlanes<float>&, int, int, int, int, void*, double*, cudaStream_t);
 template cudaError_t launch_spectrum<double>(const CPlanes<double>&, int, int, int, int, void*, double*, cudaStream_t);
 

@@ -162,6 +162,34 @@ class Solver:
                                     _stream_handle(stream)))
         return out
 
+    def ke_band_loss(self, u, kmin=4, kmax=8, ubar=None, stream=None):
+        """(L, dL/du) for L = sum_{kmin<=k<=kmax} E(k) of ke_spectrum; dL/du goes to `ubar` (allocated
+        when None)."""
+        if ubar is None:
+            ubar = self.alloc()
+        out = C.c_double()
+        check(lib().gmt_ke_band_loss(self._ctx, self._ptr(u), int(kmin), int(kmax), C.byref(out), self._ptr(ubar),
+                                     _stream_handle(stream)))
+        return out.value, ubar
+
+    # ------------------------------------------------------------------ discrete adjoint
+    def adjoint_step(self, u, ubar_next, ubar, dt, t=0.0, ch=None, glm_fac=None, do_turb=False, stream=None):
+        """ubar = (du'/du)^T ubar_next for the step u -> u' taken with the same dt, t, ch, glm_fac,
+        do_turb and forcing modes; adds the step's dL/d(turb_amp) to the context's accumulator."""
+        if ch is None:
+            ch, fac = self.glm_reference(dt)
+            glm_fac = fac if glm_fac is None else glm_fac
+        elif glm_fac is None:
+            glm_fac = self.glm_fac(ch, dt)
+        a = GmtStepArgs(float(dt), float(t), float(ch), float(glm_fac), int(bool(do_turb)), 0)
+        check(lib().gmt_adjoint_step(self._ctx, self._ptr(u), self._ptr(ubar_next), self._ptr(ubar), C.byref(a),
+                                     _stream_handle(stream)))
+
+    def adjoint_amp_grad(self, reset=True, stream=None) -> float:
+        out = C.c_double()
+        check(lib().gmt_adjoint_amp_grad(self._ctx, C.byref(out), int(bool(reset)), _stream_handle(stream)))
+        return out.value
+
     def ct_divb_max(self, q, stream=None) -> float:
         out = C.c_double()
         check(lib().gmt_ct_divb_max(self._ctx, self._ptr(q), C.byref(out), _stream_handle(stream)))

@@ -153,6 +153,24 @@ int gmt_ensemble_run(gmt_ensemble* e, void* const* u, void* const* w, int32_t ns
  * k-1/2 <= |k'| < k+1/2 of |w^(k')|^2 for k = 0..kmax (sum_k out[k] = mean kinetic energy density).
  * FP64, deterministic; the context keeps the scratch of the largest kmax used.  Synchronous. */
 int gmt_ke_spectrum(gmt_ctx* ctx, const void* u, int32_t kmax, double* out, void* stream);
+/* band-limited kinetic-energy loss L = sum_{kmin <= k <= kmax} out[k] of gmt_ke_spectrum and its
+ * gradient dL/du, written to ubar as 9 planes of u's dtype (the E, B and psi planes are zero).
+ * Synchronous. */
+int gmt_ke_band_loss(gmt_ctx* ctx, const void* u, int32_t kmin, int32_t kmax, double* loss, void* ubar, void* stream);
+
+/* --- discrete adjoint of the unsplit step (no counterpart in the reference) ----------------------
+ * ubar = (du'/du)^T ubar_next for u' = gmt_step(ctx, u, u', a): PLM reconstruction (MC or minmod),
+ * any Riemann solver, GLM, interface-state reverts, the void floor, psi damping and the forcing kick,
+ * with a->dt, a->ch, a->glm_fac and the context's current forcing table frozen at the values the
+ * forward step used (restore them with gmt_forcing_set_modes when recomputing from a checkpoint).
+ * At a limiter kink, an HLLD branch switch, a floor or a revert the derivative of the branch that
+ * the forward step took is used.  The step's part of dL/d(turb_amp) is added to an accumulator in
+ * the context (gmt_adjoint_amp_grad).  Scratch of 207 state planes is allocated on the first call.
+ * ubar must not alias u or ubar_next.  PPM and non-unsplit contexts return GMT_ERR_ARG. */
+int gmt_adjoint_step(gmt_ctx* ctx, const void* u, const void* ubar_next, void* ubar, const gmt_step_args* a,
+                     void* stream);
+/* *out = the accumulated dL/d(turb_amp); reset != 0 zeroes the accumulator afterwards.  Synchronous. */
+int gmt_adjoint_amp_grad(gmt_ctx* ctx, double* out, int32_t reset, void* stream);
 
 /* --- diagnostics without allocation --------------------------------------------------------
  * No counterpart in the reference.  Same quantities as gmt_diagnostics for a 9-plane GLM state,

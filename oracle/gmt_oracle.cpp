@@ -53,6 +53,61 @@ static int nthreads() {
 // IEEE maxNum/minNum, the same semantics as CUDA fmax/fmin and Julia's @fastmath max/min
 template <class R> static inline R rmax(R a, R b) { return std::fmax(a, b); }
 template <class R> static inline R rmin(R a, R b) { return std::fmin(a, b); }
+template <class R> static inline R osqrt(R a) { return std::sqrt(a); }
+template <class R> static inline R oabs(R a) { return std::fabs(a); }
+template <class R> static inline void set_tangent(R&, const double*) {}
+
+// Forward-mode tangents: a value and up to ORC_JVP_MAXDIR directional derivatives, for the JVP
+// entry point (the ForwardDiff counterpart of the reference's CPU step).  Every operation
+// evaluates its value exactly as the double code does; comparisons, max/min and |x| act on the
+// value, so the tangents follow the branch the value takes (at a kink, the derivative of the
+// branch taken).
+constexpr int NT = ORC_JVP_MAXDIR;
+struct Tan {
+    double v;
+    double d[NT];
+    Tan() : v(0) { for (int i = 0; i < NT; ++i) d[i] = 0; }
+    Tan(double x) : v(x) { for (int i = 0; i < NT; ++i) d[i] = 0; }
+};
+static inline Tan operator+(const Tan& a, const Tan& b) {
+    Tan r(a.v + b.v);
+    for (int i = 0; i < NT; ++i) r.d[i] = a.d[i] + b.d[i];
+    return r;
+}
+static inline Tan operator-(const Tan& a, const Tan& b) {
+    Tan r(a.v - b.v);
+    for (int i = 0; i < NT; ++i) r.d[i] = a.d[i] - b.d[i];
+    return r;
+}
+static inline Tan operator-(const Tan& a) {
+    Tan r(-a.v);
+    for (int i = 0; i < NT; ++i) r.d[i] = -a.d[i];
+    return r;
+}
+static inline Tan operator*(const Tan& a, const Tan& b) {
+    Tan r(a.v * b.v);
+    for (int i = 0; i < NT; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+    return r;
+}
+static inline Tan operator/(const Tan& a, const Tan& b) {
+    Tan r(a.v / b.v);
+    for (int i = 0; i < NT; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v;
+    return r;
+}
+static inline bool operator<(const Tan& a, const Tan& b) { return a.v < b.v; }
+static inline bool operator<=(const Tan& a, const Tan& b) { return a.v <= b.v; }
+static inline bool operator>(const Tan& a, const Tan& b) { return a.v > b.v; }
+static inline bool operator>=(const Tan& a, const Tan& b) { return a.v >= b.v; }
+static inline Tan rmax(const Tan& a, const Tan& b) { return a.v >= b.v ? a : b; }
+static inline Tan rmin(const Tan& a, const Tan& b) { return a.v <= b.v ? a : b; }
+static inline Tan osqrt(const Tan& a) {
+    Tan r(std::sqrt(a.v));
+    const double s = r.v > 0 ? 0.5 / r.v : 0.0;
+    for (int i = 0; i < NT; ++i) r.d[i] = a.d[i] * s;
+    return r;
+}
+static inline Tan oabs(const Tan& a) { return a.v >= 0 ? a : -a; }
+static inline void set_tangent(Tan& x, const double* t) { for (int i = 0; i < NT; ++i) x.d[i] = t[i]; }
 
 // ------------------------------------------------------------------------------------------
 // Parameters converted to the working precision once per call.
@@ -99,7 +154,7 @@ template <class R> static inline R fast_speed(const V9<R>& q, R gamma, R bn) {
     R c2 = gamma * q[4] / rho;
     R b2 = (q[5] * q[5] + q[6] * q[6] + q[7] * q[7]) / rho;
     R d2 = R(0.5) * (b2 + c2);
-    return std::sqrt(d2 + std::sqrt(rmax(d2 * d2 - c2 * bn * bn / rho, R(0))));
+    return osqrt(d2 + osqrt(rmax(d2 * d2 - c2 * bn * bn / rho, R(0))));
 }
 
 template <class R> static inline V9<R> phys_flux_x(const V9<R>& q, R gamma) {
@@ -136,11 +191,11 @@ template <class R> static inline V9<R> rot_from(const V9<R>& f, int d) {
 template <class R> static inline R moncen(R dl, R dr) {
     R dc = R(0.5) * (dl + dr);
     R sgn = dc >= R(0) ? R(1) : R(-1);
-    R val = sgn * rmin(R(2) * rmin(std::fabs(dl), std::fabs(dr)), std::fabs(dc));
+    R val = sgn * rmin(R(2) * rmin(oabs(dl), oabs(dr)), oabs(dc));
     return dl * dr <= R(0) ? R(0) : val;
 }
 template <class R> static inline R minmod(R a, R b) {
-    return a * b <= R(0) ? R(0) : (std::fabs(a) < std::fabs(b) ? a : b);
+    return a * b <= R(0) ? R(0) : (oabs(a) < oabs(b) ? a : b);
 }
 template <class R> static inline V9<R> slope(const V9<R>& L, const V9<R>& M, const V9<R>& Rr, bool mm) {
     V9<R> s;
@@ -182,11 +237,11 @@ template <class R> static inline V9<R> llf_x(const V9<R>& L, const V9<R>& Rr, R 
     R sL, sR;
     if (bound) {  // fast_speed_bound (glmmhd_turb.jl:307-310)
         R irL = R(1) / L[0], irR = R(1) / Rr[0];
-        sL = std::fabs(L[1]) + std::sqrt((gamma * L[4] + L[5] * L[5] + L[6] * L[6] + L[7] * L[7]) * irL);
-        sR = std::fabs(Rr[1]) + std::sqrt((gamma * Rr[4] + Rr[5] * Rr[5] + Rr[6] * Rr[6] + Rr[7] * Rr[7]) * irR);
+        sL = oabs(L[1]) + osqrt((gamma * L[4] + L[5] * L[5] + L[6] * L[6] + L[7] * L[7]) * irL);
+        sR = oabs(Rr[1]) + osqrt((gamma * Rr[4] + Rr[5] * Rr[5] + Rr[6] * Rr[6] + Rr[7] * Rr[7]) * irR);
     } else {
-        sL = std::fabs(L[1]) + fast_speed(L, gamma, L[5]);
-        sR = std::fabs(Rr[1]) + fast_speed(Rr, gamma, Rr[5]);
+        sL = oabs(L[1]) + fast_speed(L, gamma, L[5]);
+        sR = oabs(Rr[1]) + fast_speed(Rr, gamma, Rr[5]);
     }
     R smax = rmax(rmax(sL, sR), ch);
     V9<R> f;
@@ -233,12 +288,12 @@ static inline V9<R> hlld_x(const V9<R>& L, const V9<R>& Rr, R gamma, R bn, R fbn
     R pts = ((SR - uR) * dR * ptL - (SL - uL) * dL * ptR + dL * dR * (SR - uR) * (SL - uL) * (uR - uL)) / den;
     R dLs = rmax(dL * (SL - uL) / (SL - SM), tiny);
     R dRs = rmax(dR * (SR - uR) / (SR - SM), tiny);
-    R sqdLs = std::sqrt(dLs), sqdRs = std::sqrt(dRs);
-    R SLs = SM - std::fabs(bn) / sqdLs;
-    R SRs = SM + std::fabs(bn) / sqdRs;
+    R sqdLs = osqrt(dLs), sqdRs = osqrt(dRs);
+    R SLs = SM - oabs(bn) / sqdLs;
+    R SRs = SM + oabs(bn) / sqdRs;
     auto star = [&](R d, R u, R v, R w, R by, R bz, R S, R& vy, R& vz, R& byS, R& bzS) {
         R denK = d * (S - u) * (S - SM) - bn * bn;
-        if (std::fabs(denK) < tiny) {
+        if (oabs(denK) < tiny) {
             vy = v; vz = w; byS = by; bzS = bz;
         } else {
             R fac = bn * (SM - u) / denK;
@@ -376,6 +431,16 @@ struct Forcer {
         for (int q = 0; q < ORC_NMODES; ++q)
             for (int c = 0; c < 3; ++c)
                 for (int r = 0; r < 2; ++r) md[q][c][r] = (R)m[(q * 3 + c) * 2 + r];
+    }
+    // the modes scale with the forcing amplitude: tangent of a relative amplitude change
+    void seed_amplitude(const double* rel) {
+        for (int q = 0; q < ORC_NMODES; ++q)
+            for (int c = 0; c < 3; ++c)
+                for (int r = 0; r < 2; ++r) {
+                    double t[ORC_JVP_MAXDIR];
+                    for (int i = 0; i < ORC_JVP_MAXDIR; ++i) t[i] = modes[(q * 3 + c) * 2 + r] * rel[i];
+                    set_tangent(md[q][c][r], t);
+                }
     }
     void accel(int i, int j, int k, R ramp, R a[3]) const {
         const ModeTable& T = modes_table();
@@ -521,13 +586,15 @@ static inline Faces<R> recon_cell(const R* u, const Grid& g, int i, int j, int k
 // computes every face flux exactly once (the step_multi! semantics of glmmhd_turb.jl:1981-1992
 // without its N^3 scratch arrays).
 template <class R>
-static void step_unsplit(const orc_params* p, const orc_step_args* a, const R* uold, R* unew) {
+static void step_unsplit(const orc_params* p, const orc_step_args* a, const R* uold, R* unew,
+                         const double* amp_rel = nullptr) {
     Grid g(p);
     Phys<R> P(p);
     const R dx = (R)p->boxlen / (R)p->nx;
     const R dt = (R)a->dt, dtdx = dt / dx, ch = (R)a->ch, glm_fac = (R)a->glm_fac, ramp = (R)a->ramp;
     const bool turb = a->do_turb && a->modes;
     Forcer<R>* fo = turb ? new Forcer<R>(p, a->modes) : nullptr;
+    if (fo && amp_rel) fo->seed_amplitude(amp_rel);
     const int nxy = g.nx * g.ny;
     int nt = std::max(1, std::min(nthreads(), g.nz));
 #pragma omp parallel num_threads(nt)
@@ -1010,6 +1077,25 @@ void orc_accel_f64(const orc_params* p, const double* modes, double ramp, double
 
 int orc_step_unsplit_f64(const orc_params* p, const orc_step_args* a, const double* uold, double* unew) {
     step_unsplit<double>(p, a, uold, unew); return 0;
+}
+int orc_jvp_unsplit_f64(const orc_params* p, const orc_step_args* a, const double* uold, int32_t ndir,
+                        const double* duold, const double* amp_rel, double* unew, double* dunew) {
+    if (ndir < 1 || ndir > ORC_JVP_MAXDIR) return 1;
+    const size_t n = (size_t)p->nx * p->ny * p->nz * 9;
+    std::vector<Tan> in(n), out(n);
+    for (size_t i = 0; i < n; ++i) {
+        in[i] = Tan(uold[i]);
+        for (int k = 0; k < ndir; ++k) in[i].d[k] = duold ? duold[(size_t)k * n + i] : 0.0;
+    }
+    double rel[ORC_JVP_MAXDIR] = {0};
+    bool any = false;
+    for (int k = 0; k < ndir && amp_rel; ++k) { rel[k] = amp_rel[k]; any = any || rel[k] != 0.0; }
+    step_unsplit<Tan>(p, a, in.data(), out.data(), any ? rel : nullptr);
+    for (size_t i = 0; i < n; ++i) {
+        if (unew) unew[i] = out[i].v;
+        for (int k = 0; k < ndir; ++k) dunew[(size_t)k * n + i] = out[i].d[k];
+    }
+    return 0;
 }
 int orc_step_unsplit_f32(const orc_params* p, const orc_step_args* a, const float* uold, float* unew) {
     step_unsplit<float>(p, a, uold, unew); return 0;

@@ -65,6 +65,15 @@ void orc_accel_f64(const orc_params* p, const double* modes, double ramp, double
 /* unsplit PLM/PPM + MUSCL-Hancock + Riemann + GLM step (glmmhd_turb.jl:374-480, 599-767) */
 int orc_step_unsplit_f64(const orc_params* p, const orc_step_args* a, const double* uold, double* unew);
 int orc_step_unsplit_f32(const orc_params* p, const orc_step_args* a, const float* uold, float* unew);
+/* the same step evaluated on forward-mode tangents (the ForwardDiff counterpart) along ndir <=
+ * ORC_JVP_MAXDIR directions at once: dunew[k] = J duold[k] + (d unew / d amplitude) amp_rel[k],
+ * the directional derivative of the step along the state direction duold[k] (duold may be null)
+ * and the relative forcing-amplitude change amp_rel[k] (may be null; the modes scale with the
+ * amplitude).  duold and dunew hold ndir states one after another; unew (may be null) receives the
+ * ordinary FP64 step output.  Returns nonzero for an invalid ndir. */
+#define ORC_JVP_MAXDIR 8
+int orc_jvp_unsplit_f64(const orc_params* p, const orc_step_args* a, const double* uold, int32_t ndir,
+                        const double* duold, const double* amp_rel, double* unew, double* dunew);
 /* transverse-free 1-D Hancock march (spike_mhd.cu:227-302), f32 update base */
 int orc_step_march1d_f64(const orc_params* p, const orc_step_args* a, const double* uold, double* unew);
 int orc_step_march1d_f32(const orc_params* p, const orc_step_args* a, const float* uold, float* unew);

@@ -84,6 +84,8 @@ def lib():
                 f.restype = C.c_int
             getattr(L, "orc_cfl_" + nm).argtypes = [P, ptr, dp]
             getattr(L, "orc_diag_" + nm).argtypes = [P, ptr, C.POINTER(OrcDiag)]
+        L.orc_jvp_unsplit_f64.argtypes = [P, A, dp, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, dp]
+        L.orc_jvp_unsplit_f64.restype = C.c_int
         L.orc_ct_cfl_f64.argtypes = [P, dp, dp]
         L.orc_ct_divb_max_f64.argtypes = [P, dp]
         L.orc_ct_divb_max_f64.restype = C.c_double
@@ -152,6 +154,37 @@ def step_unsplit(cfg: Config, u, dt, ch, glm_fac, ramp=0.0, modes=None):
     a = _args(dt, ch, glm_fac, ramp, modes)
     _fn("orc_step_unsplit_", u)(C.byref(cfg.c()), C.byref(a), np.ascontiguousarray(u), out)
     return out
+
+
+JVP_MAXDIR = 8
+
+
+def jvp_unsplit(cfg: Config, u, du, dt, ch, glm_fac, ramp=0.0, modes=None, amp_rel=None):
+    """(step output, directional derivatives) of the FP64 unsplit step by forward-mode tangents
+    through the same code (the ForwardDiff counterpart).  `du`: one state direction or a stack
+    (k, 9, nz, ny, nx) of k <= 8, or None; `amp_rel`: relative forcing-amplitude change per
+    direction (scalar or length k), or None.  Returns dout shaped like `du` (or one state)."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    single = du is None or np.ndim(du) == u.ndim
+    if du is None:
+        k = 1 if amp_rel is None or np.ndim(amp_rel) == 0 else len(amp_rel)
+        dstack = None
+    else:
+        dstack = np.ascontiguousarray(np.asarray(du, dtype=np.float64).reshape((-1,) + u.shape))
+        k = dstack.shape[0]
+    if not 1 <= k <= JVP_MAXDIR:
+        raise ValueError("1 to 8 directions per call")
+    rel = None if amp_rel is None else np.ascontiguousarray(np.broadcast_to(np.asarray(amp_rel, dtype=np.float64), (k,)))
+    out = np.empty_like(u)
+    dout = np.empty((k,) + u.shape)
+    a = _args(dt, ch, glm_fac, ramp, modes)
+    rc = lib().orc_jvp_unsplit_f64(C.byref(cfg.c()), C.byref(a), u, k,
+                                   None if dstack is None else dstack.ctypes.data_as(C.c_void_p),
+                                   None if rel is None else rel.ctypes.data_as(C.c_void_p),
+                                   out.ctypes.data_as(C.c_void_p), dout)
+    if rc:
+        raise ValueError("orc_jvp_unsplit_f64 failed")
+    return out, (dout[0] if single else dout)
 
 
 def step_march1d(cfg: Config, u, dt, ch, glm_fac):

@@ -128,3 +128,49 @@ def test_conservation_unsplit(oracle, golden):
     r = oracle.step_unsplit(cfg, u, G.DT, G.CH, 1.0)
     for v in range(8):   # rho, momentum, E, B conserved by the flux form (psi has no source at fac=1)
         assert abs(r[v].sum() - u[v].sum()) <= 1e-12 * max(np.abs(u[v]).sum(), 1.0)
+
+
+def _generic_state(O, n, seed):
+    """Orszag-Tang plus noise on every field, so no primitive is constant along an axis (a
+    limiter kink) at the evaluation point."""
+    cfg = O.Config(n=(n, n, n), gamma=5 / 3)
+    u = O.ic_ot(cfg)
+    rng = np.random.default_rng(seed)
+    u[0] *= 1.0 + 0.1 * rng.random(u[0].shape)
+    u[1:4] += 0.05 * rng.standard_normal(u[1:4].shape)
+    u[4] *= 1.0 + 0.05 * rng.random(u[4].shape)
+    u[5:8] += 0.03 * rng.standard_normal(u[5:8].shape)
+    u[8] = 0.01 * rng.standard_normal(u[8].shape)
+    return u
+
+
+def test_oracle_jvp_matches_step_and_finite_differences(oracle):
+    """The forward-mode tangent step reproduces the FP64 step bit for bit and its directional
+    derivative agrees with central differences along a state direction and the amplitude."""
+    import math
+    O = oracle
+    n = 8
+    u = _generic_state(O, n, 3)
+    cfg = O.Config(n=(n, n, n), gamma=5 / 3, recon="mc", riemann="hlld", iflo=True)
+    f = O.OUForcing(amp=2.0, T=0.5, ndt=100, seed=0)
+    f.advance()
+    cmax, smax = O.cfl(cfg, u)
+    dt = 0.3 * cfg.dx / cmax
+    fac = math.exp(-(smax / 0.18) * dt)
+    kw = dict(ramp=0.4, modes=f.modes)
+    rng = np.random.default_rng(4)
+    v = rng.standard_normal(u.shape) * np.abs(u).max(axis=(1, 2, 3), keepdims=True)
+    v[0] *= 0.1
+    v[4] *= 0.1
+    out, jv = O.jvp_unsplit(cfg, u, v, dt, smax, fac, **kw)
+    np.testing.assert_array_equal(out, O.step_unsplit(cfg, u, dt, smax, fac, **kw))
+    eps = 1e-8
+    fd = (O.step_unsplit(cfg, u + eps * v, dt, smax, fac, **kw) - O.step_unsplit(cfg, u - eps * v, dt, smax, fac, **kw)) / (2 * eps)
+    assert np.abs(fd - jv).max() <= 1e-5 * np.abs(jv).max()
+    # amplitude direction: the modes scale with the amplitude
+    _, ja = O.jvp_unsplit(cfg, u, None, dt, smax, fac, amp_rel=1.0, **kw)
+    ea = 1e-6
+    fa = (O.step_unsplit(cfg, u, dt, smax, fac, ramp=0.4, modes=f.modes * (1 + ea)) -
+          O.step_unsplit(cfg, u, dt, smax, fac, ramp=0.4, modes=f.modes * (1 - ea))) / (2 * ea)
+    assert np.abs(fa - ja).max() <= 1e-5 * np.abs(ja).max()   # FD roundoff ~1e-16/ea
+    assert np.abs(ja[[0, 5, 6, 7, 8]]).max() == 0.0   # the kick moves momentum and energy only
