@@ -31,7 +31,7 @@ EXPORTS = (
     "gmt_forcing_reset", "gmt_forcing_advance", "gmt_forcing_set_modes", "gmt_forcing_get_modes",
     "gmt_forcing_counter", "gmt_ic_orszag_tang", "gmt_ic_uniform", "gmt_ic_turbulent", "gmt_ct_step", "gmt_ct_cfl_async",
     "gmt_ct_divb_max", "gmt_ct_ic_orszag_tang", "gmt_ke_spectrum", "gmt_run", "gmt_ensemble_create", "gmt_ensemble_destroy",
-    "gmt_ensemble_run", "gmt_ke_band_loss", "gmt_adjoint_step", "gmt_adjoint_amp_grad", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
+    "gmt_ensemble_run", "gmt_density_pdf", "gmt_ke_band_loss", "gmt_adjoint_step", "gmt_adjoint_amp_grad", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
     "march_set_glm", "march_set_gamma", "march_run_dev", "march_set_nx", "ct_run", "ct_regs", "ct_shmem",
 )
 
@@ -40,7 +40,7 @@ class GmtParams(C.Structure):
     _fields_ = [("abi_version", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
                 ("dtype", C.c_int32), ("scheme", C.c_int32), ("recon", C.c_int32), ("riemann", C.c_int32),
                 ("iflo", C.c_int32), ("emf", C.c_int32), ("ct_halfslope", C.c_int32),
-                ("tile_x", C.c_int32), ("tile_y", C.c_int32), ("tile_z", C.c_int32), ("pad0", C.c_int32),
+                ("tile_x", C.c_int32), ("tile_y", C.c_int32), ("tile_z", C.c_int32), ("nsp", C.c_int32),
                 ("boxlen", C.c_double), ("gamma", C.c_double), ("courant", C.c_double),
                 ("smallr", C.c_double), ("smallc", C.c_double), ("smallp", C.c_double),
                 ("glm_ch_scale", C.c_double), ("glm_cp_coef", C.c_double), ("llf_dmin", C.c_double),
@@ -105,6 +105,7 @@ def lib():
             "gmt_ct_ic_orszag_tang": ([vp, vp, vp], C.c_int),
             "gmt_ke_spectrum": ([vp, vp, i32, C.POINTER(dbl), vp], C.c_int),
             "gmt_ke_band_loss": ([vp, vp, i32, i32, C.POINTER(dbl), vp, vp], C.c_int),
+            "gmt_density_pdf": ([vp, vp, i32, dbl, dbl, C.POINTER(dbl), C.POINTER(dbl), vp], C.c_int),
             "gmt_adjoint_step": ([vp, vp, vp, vp, A, vp], C.c_int),
             "gmt_adjoint_amp_grad": ([vp, C.POINTER(dbl), i32, vp], C.c_int),
             "gmt_run": ([vp, vp, vp, i32, dbl, dbl, i32, vp, C.POINTER(dbl), C.POINTER(i32)], C.c_int),

@@ -31,7 +31,7 @@ def save(path: str, u: torch.Tensor, *, t: float = 0.0, step: int = 0, solver: S
               "next_time": float(solver.next_time) if solver is not None else 0.0, "extra": extra or {}}
     if solver is not None:
         p = solver.params
-        header["params"] = {k: getattr(p, k) for k, _ in p._fields_ if k != "pad0"}
+        header["params"] = {k: getattr(p, k) for k, _ in p._fields_}
     hb = json.dumps(header).encode()
     with open(path, "wb") as f:
         f.write(MAGIC)

@@ -146,7 +146,8 @@ template <class R> Planes<R> planes(void* base, size_t n) {
 }
 
 template <class R>
-int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_step_args* a, cudaStream_t s) {
+int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_step_args* a, cudaStream_t s,
+              const void* const* sp_in = nullptr, void* const* sp_out = nullptr) {
     const gmt_params& p = c->p;
     const double dx = p.boxlen / p.nx;
     if (!(a->dt > 0.0) || !std::isfinite(a->dt)) return fail(GMT_ERR_ARG, "dt must be positive and finite");
@@ -185,6 +186,14 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.ch = (R)a->ch; A.glm_fac = (R)a->glm_fac;
         A.K = consts_of<R>(p);
         A.ppm = p.recon == GMT_RECON_PPM;
+        A.nsp = p.nsp;
+        for (int k = 0; k < MAX_SPECIES; ++k) { A.su[k] = nullptr; A.so[k] = nullptr; }
+        if (p.nsp > 0 && (!sp_in || !sp_out)) return fail(GMT_ERR_ARG, "gmt_step: species planes missing");
+        for (int k = 0; k < p.nsp; ++k) {
+            A.su[k] = static_cast<const R*>(sp_in[k]);
+            A.so[k] = static_cast<R*>(sp_out[k]);
+            if (!A.su[k] || !A.so[k]) return fail(GMT_ERR_ARG, "gmt_step: null species plane");
+        }
         cudaError_t e = launch_march1d(A, s);
         if (e != cudaSuccess) return cuda_fail(e, "march1d step");
         if (a->want_cfl) {
@@ -292,6 +301,9 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     if (p->scheme < 0 || p->scheme > 2) return fail(GMT_ERR_ARG, "gmt_create: unknown scheme");
     if (p->recon < 0 || p->recon > 2) return fail(GMT_ERR_ARG, "gmt_create: unknown recon");
     if (p->riemann < 0 || p->riemann > 3) return fail(GMT_ERR_ARG, "gmt_create: unknown riemann");
+    if (p->nsp < 0 || p->nsp > GMT_MAX_SPECIES) return fail(GMT_ERR_ARG, "gmt_create: nsp must be 0..GMT_MAX_SPECIES");
+    if (p->nsp > 0 && p->scheme != GMT_SCHEME_MARCH1D)
+        return fail(GMT_ERR_UNSUPPORTED, "gmt_create: passive species ride the march scheme (spike_mhd.cu NSP)");
     if (p->scheme == GMT_SCHEME_MARCH1D && p->riemann != GMT_RIEMANN_HLL)
         return fail(GMT_ERR_UNSUPPORTED, "gmt_create: the march scheme uses HLL (spike_mhd.cu:199-223)");
     if (p->scheme == GMT_SCHEME_CT && p->riemann != GMT_RIEMANN_HLL && p->riemann != GMT_RIEMANN_HLLD)
@@ -421,8 +433,15 @@ int gmt_step(gmt_ctx* c, const void* uold, void* unew, const gmt_step_args* a, v
     if (!c || !uold || !unew || !a) return fail(GMT_ERR_ARG, "gmt_step: null argument");
     if (uold == unew) return fail(GMT_ERR_ARG, "gmt_step: uold and unew must be different buffers");
     cudaStream_t s = (cudaStream_t)stream;
-    if (c->esize == 8) return step_impl<double>(c, cplanes<double>(uold, c->n), planes<double>(unew, c->n), a, s);
-    return step_impl<float>(c, cplanes<float>(uold, c->n), planes<float>(unew, c->n), a, s);
+    const void* si[MAX_SPECIES];
+    void* so[MAX_SPECIES];
+    for (int k = 0; k < c->p.nsp; ++k) {
+        si[k] = static_cast<const char*>(uold) + (size_t)(9 + k) * c->n * c->esize;
+        so[k] = static_cast<char*>(unew) + (size_t)(9 + k) * c->n * c->esize;
+    }
+    if (c->esize == 8)
+        return step_impl<double>(c, cplanes<double>(uold, c->n), planes<double>(unew, c->n), a, s, si, so);
+    return step_impl<float>(c, cplanes<float>(uold, c->n), planes<float>(unew, c->n), a, s, si, so);
 }
 
 int gmt_step_planes(gmt_ctx* c, const void* const* uold, void* const* unew, const gmt_step_args* a, void* stream) {
@@ -433,11 +452,11 @@ int gmt_step_planes(gmt_ctx* c, const void* const* uold, void* const* unew, cons
     if (c->esize == 8) {
         CPlanes<double> u; Planes<double> o;
         for (int v = 0; v < 9; ++v) { u.p[v] = (const double*)uold[v]; o.p[v] = (double*)unew[v]; }
-        return step_impl<double>(c, u, o, a, s);
+        return step_impl<double>(c, u, o, a, s, uold + 9, unew + 9);
     }
     CPlanes<float> u; Planes<float> o;
     for (int v = 0; v < 9; ++v) { u.p[v] = (const float*)uold[v]; o.p[v] = (float*)unew[v]; }
-    return step_impl<float>(c, u, o, a, s);
+    return step_impl<float>(c, u, o, a, s, uold + 9, unew + 9);
 }
 
 int gmt_cfl_async(gmt_ctx* c, const void* u, void* stream) {
@@ -519,6 +538,27 @@ int gmt_ke_spectrum(gmt_ctx* c, const void* u, int32_t kmax, double* out, void* 
                         ? launch_spectrum<double>(cplanes<double>(u, c->n), c->p.nx, c->p.ny, c->p.nz, kmax, c->spec, out, s)
                         : launch_spectrum<float>(cplanes<float>(u, c->n), c->p.nx, c->p.ny, c->p.nz, kmax, c->spec, out, s);
     return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_ke_spectrum");
+}
+
+int gmt_density_pdf(gmt_ctx* c, const void* u, int32_t nbins, double smin, double smax, double* pdf, double stats[3],
+                    void* stream) {
+    if (!c || !u || !pdf || !stats) return fail(GMT_ERR_ARG, "gmt_density_pdf: null argument");
+    if (nbins < 1 || nbins > GMT_PDF_MAX_BINS) return fail(GMT_ERR_ARG, "gmt_density_pdf: nbins must be 1..4096");
+    if (!(smax > smin) || !std::isfinite(smin) || !std::isfinite(smax))
+        return fail(GMT_ERR_ARG, "gmt_density_pdf: need finite smin < smax");
+    size_t need = pdf_scratch_bytes(nbins);
+    if (need > c->spec_bytes) {
+        cudaFree(c->spec);
+        c->spec = nullptr;
+        c->spec_bytes = 0;
+        GMT_CUDA(cudaMalloc(&c->spec, need));
+        c->spec_bytes = need;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = c->esize == 8
+        ? launch_density_pdf<double>(static_cast<const double*>(u), c->n, nbins, smin, smax, c->spec, pdf, stats, s)
+        : launch_density_pdf<float>(static_cast<const float*>(u), c->n, nbins, smin, smax, c->spec, pdf, stats, s);
+    return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_density_pdf");
 }
 
 int gmt_ke_band_loss(gmt_ctx* c, const void* u, int32_t kmin, int32_t kmax, double* loss, void* ubar, void* stream) {
@@ -1166,6 +1206,9 @@ int gmt_ct_ic_orszag_tang(gmt_ctx* c, void* q, void* stream) {
 // legacy bridge ABI: __constant__-style setters become process-wide state (spike_mhd.cu:52,
 // 321-340); each grid size gets its own lazily created FP32 context.
 // ------------------------------------------------------------------------------------------
+#ifndef GMT_LEGACY_NSP
+#define GMT_LEGACY_NSP 0     // passive species of the legacy march build (spike_mhd.cu -DNSP)
+#endif
 #ifndef GMT_LEGACY_NX
 #define GMT_LEGACY_NX 480
 #endif
@@ -1187,15 +1230,16 @@ static gmt_ctx* legacy_ctx(int which) {
         p.smallr = 1e-6;
         p.smallp = 1e-6;
         p.boxlen = 1.0;
+        if (which == 0) p.nsp = GMT_LEGACY_NSP;
         if (gmt_create(&p, &c) != GMT_OK) c = nullptr;
         g_legacy_gamma_of[which] = g_gamma;
     }
     return c;
 }
 
-int march_nv(void) { return 9; }
+int march_nv(void) { return 9 + GMT_LEGACY_NSP; }
 int march_nx(void) { return g_legacy_nx; }
-int march_nsp(void) { return 0; }
+int march_nsp(void) { return GMT_LEGACY_NSP; }
 void march_set_nx(int n) {
     std::lock_guard<std::mutex> lk(g_legacy_mu);
     if (n > 0) g_legacy_nx = n;
@@ -1213,9 +1257,10 @@ double march_run_dev(float* const* qv, float* const* ov, int nsteps) {
     a.dt = (double)g_dtdx * dx;
     a.ch = g_ch;
     a.glm_fac = g_glmfac;
-    const void* q[9];
-    void* o[9];
-    for (int v = 0; v < 9; ++v) { q[v] = qv[v]; o[v] = ov[v]; }
+    constexpr int NV = 9 + GMT_LEGACY_NSP;
+    const void* q[NV];
+    void* o[NV];
+    for (int v = 0; v < NV; ++v) { q[v] = qv[v]; o[v] = ov[v]; }
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
@@ -1232,7 +1277,7 @@ double march_run_dev(float* const* qv, float* const* ov, int nsteps) {
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (!in_q)
-        for (int v = 0; v < 9; ++v) cudaMemcpy(qv[v], ov[v], c->n * sizeof(float), cudaMemcpyDeviceToDevice);
+        for (int v = 0; v < NV; ++v) cudaMemcpy(qv[v], ov[v], c->n * sizeof(float), cudaMemcpyDeviceToDevice);
     return (double)ms;
 }
 

@@ -26,6 +26,7 @@ size_t unsplit_smem(int dtype_bytes, int ox, int oy);
 int unsplit_regs(int dtype_bytes, int recon, int riem, int nthreads);
 
 // transverse-free 1-D Hancock march (gmt_march1d.cu)
+constexpr int MAX_SPECIES = 8;
 template <class R> struct MarchArgs {
     CPlanes<R> u;
     Planes<R> o;
@@ -33,6 +34,9 @@ template <class R> struct MarchArgs {
     R dtdx, ch, glm_fac;
     Consts<R> K;
     int ppm;
+    int nsp;                       // passive species: su[s] = rho*X in, so[s] out
+    const R* su[MAX_SPECIES];
+    R* so[MAX_SPECIES];
 };
 cudaError_t launch_march1d(const MarchArgs<float>& A, cudaStream_t s);
 cudaError_t launch_march1d(const MarchArgs<double>& A, cudaStream_t s);
@@ -79,6 +83,9 @@ size_t spectrum_scratch_bytes(int nx, int ny, int nz, int kmax);
 template <class R> cudaError_t launch_spectrum(const CPlanes<R>& u, int nx, int ny, int nz, int kmax, void* scratch,
                                                double* E_host, cudaStream_t s);
 size_t band_scratch_bytes(int nx, int ny, int nz, int kmax);
+size_t pdf_scratch_bytes(int nbins);
+template <class R> cudaError_t launch_density_pdf(const R* rho, size_t n, int nbins, double smin, double smax,
+                                                  void* scratch, double* pdf_host, double* stats_host, cudaStream_t s);
 template <class R> cudaError_t launch_band_loss(const CPlanes<R>& u, int nx, int ny, int nz, int kmin, int kmax,
                                                 void* scratch, double* L_host, const Planes<R>& ub, cudaStream_t s);
 // discrete adjoint of one unsplit PLM step, dt frozen (gmt_adjoint.cu)

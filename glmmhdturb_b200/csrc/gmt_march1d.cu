@@ -5,6 +5,11 @@
 // mh +- s/2 (or Julia-form PPM edges + predictor shift, glmmhd_turb.jl:917-926), HLL with GLM
 // cleaning, then u -= dt/dx * sum_d (F_hi - F_lo) and psi *= glmfac.  The update base is the
 // state read from HBM (the spike adds the increment to a 16-bit tile copy instead).
+//
+// Passive species (spike_mhd.cu:55-61, 128-139, 155-158, 218-221, 241-244, 278-296): planes hold
+// rho*X; the fraction X = rho*X / max(rho, smallr) gets the same full MonCen slope, the predictor
+// X - dt/(2dx) u_n dX and the faces X_h +- s/2 (or the PPM edge + predictor shift), and rides the
+// face mass flux: F_X = F_rho X_L if F_rho >= 0, else F_rho X_R (consistent multi-fluid advection).
 #include "gmt_internal.h"
 
 namespace gmt {
@@ -38,6 +43,26 @@ __device__ __forceinline__ Q9<R> march_face(const Q9<R>& m2, const Q9<R>& m1, co
     return rot_from<D>(hll_x(Lr, Rrr, K.gamma, bns, psis, ch * ch * bns));
 }
 
+// species flux at the face between cells m1 and c0 (stencil m2, m1 | c0, p1 along the direction)
+template <class R>
+__device__ __forceinline__ R species_face(R xm2, R xm1, R xc0, R xp1, R un_m1, R un_c0, R h, R frho, bool ppm) {
+    R sL = full_mc(xm2, xm1, xc0), sR = full_mc(xm1, xc0, xp1);
+    R mhL = xm1 - h * un_m1 * sL;
+    R mhR = xc0 - h * un_c0 * sR;
+    R L, Rr;
+    if (ppm) {
+        R lo, hi;
+        ppm_edges(xm2, xm1, xc0, lo, hi);
+        L = hi + mhL - xm1;
+        ppm_edges(xm1, xc0, xp1, lo, hi);
+        Rr = lo + mhR - xc0;
+    } else {
+        L = mhL + R(0.5) * sL;
+        Rr = mhR + R(-0.5) * sR;
+    }
+    return frho >= R(0) ? frho * L : frho * Rr;
+}
+
 template <class R>
 __device__ __forceinline__ Q9<R> prim_at(const CPlanes<R>& u, size_t g, const Consts<R>& K) {
     Q9<R> c;
@@ -47,7 +72,7 @@ __device__ __forceinline__ Q9<R> prim_at(const CPlanes<R>& u, size_t g, const Co
 }
 
 template <int D, class R>
-__device__ __forceinline__ void march_dir(const MarchArgs<R>& A, int x, int y, int z, Q9<R>& div) {
+__device__ __forceinline__ void march_dir(const MarchArgs<R>& A, int x, int y, int z, Q9<R>& div, R* divs) {
     auto at = [&](int s) {
         int xx = x + (D == 0 ? s : 0), yy = y + (D == 1 ? s : 0), zz = z + (D == 2 ? s : 0);
         return (size_t)wrapi(xx, A.nx) + (size_t)A.nx * ((size_t)wrapi(yy, A.ny) + (size_t)A.ny * wrapi(zz, A.nz));
@@ -58,6 +83,22 @@ __device__ __forceinline__ void march_dir(const MarchArgs<R>& A, int x, int y, i
     Q9<R> Fp = march_face<D>(cm1, c0, cp1, cp2, A.K, A.dtdx, A.ch, A.ppm != 0);
 #pragma unroll
     for (int v = 0; v < 9; ++v) div.v[v] = div.v[v] + (Fp.v[v] - Fm.v[v]);
+    if (A.nsp > 0) {
+        const size_t g[5] = {at(-2), at(-1), at(0), at(1), at(2)};
+        const R rho[5] = {cm2.v[0], cm1.v[0], c0.v[0], cp1.v[0], cp2.v[0]};
+        const R h = R(0.5) * A.dtdx;
+#pragma unroll
+        for (int s = 0; s < MAX_SPECIES; ++s) {
+            if (s < A.nsp) {
+                R X[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) X[k] = A.su[s][g[k]] / rho[k];
+                R fm = species_face(X[0], X[1], X[2], X[3], cm1.v[1 + D], c0.v[1 + D], h, Fm.v[0], A.ppm != 0);
+                R fp = species_face(X[1], X[2], X[3], X[4], c0.v[1 + D], cp1.v[1 + D], h, Fp.v[0], A.ppm != 0);
+                divs[s] = divs[s] + (fp - fm);
+            }
+        }
+    }
 }
 
 template <class R>
@@ -66,17 +107,23 @@ __global__ void __launch_bounds__(128) march1d_kernel(const MarchArgs<R> A) {
     for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
         int x = (int)(g % A.nx), y = (int)((g / A.nx) % A.ny), z = (int)(g / ((size_t)A.nx * A.ny));
         Q9<R> div;
+        R divs[MAX_SPECIES];
 #pragma unroll
         for (int v = 0; v < 9; ++v) div.v[v] = R(0);
-        march_dir<0>(A, x, y, z, div);
-        march_dir<1>(A, x, y, z, div);
-        march_dir<2>(A, x, y, z, div);
+#pragma unroll
+        for (int s = 0; s < MAX_SPECIES; ++s) divs[s] = R(0);
+        march_dir<0>(A, x, y, z, div, divs);
+        march_dir<1>(A, x, y, z, div, divs);
+        march_dir<2>(A, x, y, z, div, divs);
 #pragma unroll
         for (int v = 0; v < 9; ++v) {
             R u = A.u.p[v][g] - A.dtdx * div.v[v];
             if (v == 8) u = u * A.glm_fac;
             A.o.p[v][g] = u;
         }
+#pragma unroll
+        for (int s = 0; s < MAX_SPECIES; ++s)
+            if (s < A.nsp) A.so[s][g] = A.su[s][g] - A.dtdx * divs[s];
     }
 }
 

@@ -308,6 +308,108 @@ template cudaError_t launch_band_loss<float>(const CPlanes<float>&, int, int, in
 template cudaError_t launch_band_loss<double>(const CPlanes<double>&, int, int, int, int, int, void*, double*,
                                               const Planes<double>&, cudaStream_t);
 
+// ---------------------------------------------------------------------------------------------
+// Log-density PDF: s = ln(rho / <rho>), its histogram on [smin, smax) and its mean and standard
+// deviation sigma_s.  Per-block FP64 partials in a fixed tree order and a one-thread final sum
+// (deterministic); the histogram is integer counts.
+// ---------------------------------------------------------------------------------------------
+constexpr int PDF_BLOCKS = 592, PDF_THREADS = 256;
+
+template <class R>
+__device__ __forceinline__ double block_sum256(double v, double* red) {
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int st = PDF_THREADS / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
+    double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+template <class R>
+__global__ void __launch_bounds__(PDF_THREADS) pdf_mass_kernel(const R* rho, size_t n, double* part) {
+    __shared__ double red[PDF_THREADS];
+    double m = 0.0;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+        m += (double)rho[c];
+    double t = block_sum256<R>(m, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void pdf_mean_kernel(const double* part, int nb, size_t n, double* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double m = 0.0;
+    for (int b = 0; b < nb; ++b) m += part[b];
+    out[0] = m / (double)n;
+}
+
+template <class R>
+__global__ void __launch_bounds__(PDF_THREADS) pdf_hist_kernel(const R* rho, size_t n, const double* mean, int nbins,
+                                                               double smin, double smax, double* part,
+                                                               unsigned long long* hist) {
+    __shared__ double red[PDF_THREADS];
+    extern __shared__ unsigned int hs[];
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) hs[b] = 0u;
+    __syncthreads();
+    const double irm = 1.0 / mean[0];
+    const double idel = (double)nbins / (smax - smin);
+    double s1 = 0.0, s2 = 0.0;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        double sv = log((double)rho[c] * irm);
+        s1 += sv;
+        s2 += sv * sv;
+        double f = (sv - smin) * idel;
+        if (f >= 0.0 && f < (double)nbins) atomicAdd(&hs[(int)f], 1u);
+    }
+    double t1 = block_sum256<R>(s1, red);
+    double t2 = block_sum256<R>(s2, red);
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = t1; part[2 * blockIdx.x + 1] = t2; }
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+        if (hs[b]) atomicAdd(&hist[b], (unsigned long long)hs[b]);
+}
+
+__global__ void pdf_final_kernel(const double* part, int nb, size_t n, double* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double s1 = 0.0, s2 = 0.0;
+    for (int b = 0; b < nb; ++b) { s1 += part[2 * b]; s2 += part[2 * b + 1]; }
+    const double m = s1 / (double)n;
+    out[1] = m;
+    out[2] = sqrt(fmax(s2 / (double)n - m * m, 0.0));
+}
+
+size_t pdf_scratch_bytes(int nbins) { return (size_t)(3 * PDF_BLOCKS + 8) * sizeof(double) + (size_t)nbins * 8; }
+
+template <class R>
+cudaError_t launch_density_pdf(const R* rho, size_t n, int nbins, double smin, double smax, void* scratch,
+                               double* pdf_host, double* stats_host, cudaStream_t s) {
+    double* part = static_cast<double*>(scratch);          // [3 * PDF_BLOCKS]
+    double* out = part + 3 * PDF_BLOCKS;                    // [mean rho, mean s, sigma_s]
+    unsigned long long* hist = reinterpret_cast<unsigned long long*>(out + 8);
+    cudaError_t e = cudaMemsetAsync(hist, 0, (size_t)nbins * 8, s);
+    if (e != cudaSuccess) return e;
+    pdf_mass_kernel<R><<<PDF_BLOCKS, PDF_THREADS, 0, s>>>(rho, n, part);
+    pdf_mean_kernel<<<1, 1, 0, s>>>(part, PDF_BLOCKS, n, out);
+    pdf_hist_kernel<R><<<PDF_BLOCKS, PDF_THREADS, (size_t)nbins * sizeof(unsigned), s>>>(rho, n, out, nbins, smin, smax,
+                                                                                        part, hist);
+    pdf_final_kernel<<<1, 1, 0, s>>>(part, PDF_BLOCKS, n, out);
+    e = cudaGetLastError();
+    std::vector<unsigned long long> h((size_t)nbins);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), hist, (size_t)nbins * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(stats_host, out, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    const double ds = (smax - smin) / nbins;
+    for (int b = 0; b < nbins; ++b) pdf_host[b] = (double)h[b] / ((double)n * ds);
+    return cudaSuccess;
+}
+
+template cudaError_t launch_density_pdf<float>(const float*, size_t, int, double, double, void*, double*, double*,
+                                               cudaStream_t);
+template cudaError_t launch_density_pdf<double>(const double*, size_t, int, double, double, void*, double*, double*,
+                                                cudaStream_t);
+
 template cudaError_t launch_spectrum<float>(const CPlanes<float>&, int, int, int, int, void*, double*, cudaStream_t);
 template cudaError_t launch_spectrum<double>(const CPlanes<double>&, int, int, int, int, void*, double*, cudaStream_t);
 

@@ -33,7 +33,7 @@ class Solver:
     def __init__(self, n, *, dtype="f32", scheme="unsplit", recon="mc", riemann="hlld", iflo=True,
                  emf="average", ct_halfslope=False, boxlen=1.0, gamma=1.01, courant=0.7, smallr=1e-6,
                  smallc=1e-4, smallp=1e-6, glm_ch_scale=0.25, glm_cp_coef=0.18, llf_dmin=0.0, llf_pmin=0.0,
-                 turb_min_rho=1e-5, turb_amp=0.0, turb_T=0.3, turb_ndt=100, turb_seed=1, tile=(0, 0, 0)):
+                 turb_min_rho=1e-5, turb_amp=0.0, turb_T=0.3, turb_ndt=100, turb_seed=1, tile=(0, 0, 0), nsp=0):
         if isinstance(n, int):
             n = (n, n, n)
         self.nx, self.ny, self.nz = (int(v) for v in n)
@@ -42,7 +42,8 @@ class Solver:
         self.dtype_name = dtype
         self.code, self.torch_dtype = _DT[dtype]
         self.scheme = scheme
-        self.nvar = 8 if scheme == "ct" else 9
+        self.nsp = int(nsp)   # march scheme: passive species planes (rho*X) after the 9 MHD planes
+        self.nvar = 8 if scheme == "ct" else 9 + self.nsp
         p = GmtParams()
         check(lib().gmt_params_init(C.byref(p), self.nx))
         p.nx, p.ny, p.nz = self.nx, self.ny, self.nz
@@ -54,6 +55,7 @@ class Solver:
         p.emf = _lib.EMF[emf]
         p.ct_halfslope = int(bool(ct_halfslope))
         p.tile_x, p.tile_y, p.tile_z = (int(v) for v in tile)
+        p.nsp = self.nsp
         p.boxlen, p.gamma, p.courant = boxlen, gamma, courant
         p.smallr, p.smallc, p.smallp = smallr, smallc, smallp
         p.glm_ch_scale, p.glm_cp_coef = glm_ch_scale, glm_cp_coef
@@ -161,6 +163,16 @@ class Solver:
         check(lib().gmt_ke_spectrum(self._ctx, self._ptr(u), int(kmax), out.ctypes.data_as(C.POINTER(C.c_double)),
                                     _stream_handle(stream)))
         return out
+
+    def density_pdf(self, u, nbins=64, smin=-4.0, smax=4.0, stream=None):
+        """(pdf, stats) of s = ln(rho/<rho>): pdf per bin of [smin, smax) (density, FP64) and
+        stats = {'rho_mean', 's_mean', 'sigma_s'}."""
+        pdf = np.zeros(int(nbins))
+        st = np.zeros(3)
+        check(lib().gmt_density_pdf(self._ctx, self._ptr(u), int(nbins), float(smin), float(smax),
+                                    pdf.ctypes.data_as(C.POINTER(C.c_double)), st.ctypes.data_as(C.POINTER(C.c_double)),
+                                    _stream_handle(stream)))
+        return pdf, {"rho_mean": st[0], "s_mean": st[1], "sigma_s": st[2]}
 
     def ke_band_loss(self, u, kmin=4, kmax=8, ubar=None, stream=None):
         """(L, dL/du) for L = sum_{kmin<=k<=kmax} E(k) of ke_spectrum; dL/du goes to `ubar` (allocated

@@ -31,6 +31,7 @@ extern "C" {
 #endif
 
 #define GMT_ABI_VERSION 1
+#define GMT_MAX_SPECIES 8
 
 /* status codes (0 = success) */
 enum {
@@ -61,7 +62,8 @@ typedef struct gmt_params {
     int32_t emf;              /* CT edge EMF: GMT_EMF_* */
     int32_t ct_halfslope;     /* CT: 1 = ct_mhd.jl's extra factor 1/2 on the slope (:49-50) */
     int32_t tile_x, tile_y, tile_z; /* 0 = automatic */
-    int32_t pad0;
+    int32_t nsp;              /* march scheme: passive species (0..GMT_MAX_SPECIES); planes 9.. of the
+                               * state hold rho*X, carried by the face mass flux (spike_mhd.cu:218-221) */
     double boxlen, gamma, courant, smallr, smallc;
     double smallp;            /* march / CT pressure floor (spike_mhd.cu:52) */
     double glm_ch_scale, glm_cp_coef;
@@ -103,9 +105,9 @@ int gmt_destroy(gmt_ctx* ctx);
 int gmt_kernel_info(gmt_ctx* ctx, int32_t* regs, int64_t* smem_bytes, int32_t tile[3]);
 
 /* --- GLM step (unsplit: step_plm!/step_tiled!/step_multi!; march1d: march_run_dev) ------- */
-/* uold/unew: base pointers of 9 contiguous planes (plane stride nx*ny*nz) */
+/* uold/unew: base pointers of 9 contiguous planes (plane stride nx*ny*nz), 9 + nsp with species */
 int gmt_step(gmt_ctx* ctx, const void* uold, void* unew, const gmt_step_args* a, void* stream);
-/* same with one pointer per plane (the bridge's float*[9] layout) */
+/* same with one pointer per plane (the bridge's float*[9 + nsp] layout) */
 int gmt_step_planes(gmt_ctx* ctx, const void* const* uold, void* const* unew, const gmt_step_args* a,
                     void* stream);
 
@@ -153,6 +155,12 @@ int gmt_ensemble_run(gmt_ensemble* e, void* const* u, void* const* w, int32_t ns
  * k-1/2 <= |k'| < k+1/2 of |w^(k')|^2 for k = 0..kmax (sum_k out[k] = mean kinetic energy density).
  * FP64, deterministic; the context keeps the scratch of the largest kmax used.  Synchronous. */
 int gmt_ke_spectrum(gmt_ctx* ctx, const void* u, int32_t kmax, double* out, void* stream);
+/* log-density statistics of a GLM state: s = ln(rho/<rho>); pdf[b] = fraction of cells with s in bin b
+ * of [smin, smax) divided by the bin width (nbins <= 4096); stats = {<rho>, <s>, sigma_s}.  FP64,
+ * deterministic; synchronous. */
+#define GMT_PDF_MAX_BINS 4096
+int gmt_density_pdf(gmt_ctx* ctx, const void* u, int32_t nbins, double smin, double smax, double* pdf, double stats[3],
+                    void* stream);
 /* band-limited kinetic-energy loss L = sum_{kmin <= k <= kmax} out[k] of gmt_ke_spectrum and its
  * gradient dL/du, written to ubar as 9 planes of u's dtype (the E, B and psi planes are zero).
  * Synchronous. */

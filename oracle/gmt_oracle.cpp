@@ -677,15 +677,16 @@ static inline V9<R> hanc1d(const V9<R>& c0, const V9<R>& s, int d, R dtdx, R gam
     for (int v = 0; v < 9; ++v) U[v] = U[v] - h * (FR[v] - FL[v]);
     return prim_from_cons_floor(U, gamma, smallr, smallp);
 }
+// spike moncen(a,b,c) = sgn*min(|dc|, 2|dl|, 2|dr|), dc = (c-a)/2  (full slope)
+template <class R> static inline R full_mc(R a, R b, R c) {
+    R dl = b - a, dr = c - b, dc = R(0.5) * (c - a);
+    if (dl * dr <= R(0)) return R(0);
+    R sg = dl > R(0) ? R(1) : R(-1);
+    return sg * rmin(std::fabs(dc), rmin(R(2) * std::fabs(dl), R(2) * std::fabs(dr)));
+}
 template <class R> static inline V9<R> full_slope(const V9<R>& a, const V9<R>& b, const V9<R>& c) {
-    // spike moncen(a,b,c) = sgn*min(|dc|, 2|dl|, 2|dr|), dc = (c-a)/2  (full slope)
     V9<R> s;
-    for (int v = 0; v < 9; ++v) {
-        R dl = b[v] - a[v], dr = c[v] - b[v], dc = R(0.5) * (c[v] - a[v]);
-        if (dl * dr <= R(0)) { s[v] = R(0); continue; }
-        R sg = dl > R(0) ? R(1) : R(-1);
-        s[v] = sg * rmin(std::fabs(dc), rmin(R(2) * std::fabs(dl), R(2) * std::fabs(dr)));
-    }
+    for (int v = 0; v < 9; ++v) s[v] = full_mc(a[v], b[v], c[v]);
     return s;
 }
 // one lower-face flux in direction d from 4 cells along d (m2, m1 | c0, p1)
@@ -720,6 +721,29 @@ static inline V9<R> march_face(const V9<R>& m2, const V9<R>& m1, const V9<R>& c0
     return rot_from(f, d);
 }
 
+// Passive species (spike_mhd.cu:55-61, 128-139, 155-158, 218-221, 241-244, 278-296): the fraction
+// X = rho*X / max(rho, smallr) gets the full MonCen slope, the predictor X - dt/(2dx) u_n dX and the
+// faces X_h +- s/2 (or the PPM edge + predictor shift), and rides the face mass flux (consistent
+// multi-fluid advection): F_X = F_rho X_L if F_rho >= 0, else F_rho X_R.
+template <class R>
+static inline R species_face(R xm2, R xm1, R xc0, R xp1, R un_m1, R un_c0, R h, R frho, bool ppm) {
+    R sL = full_mc(xm2, xm1, xc0), sR = full_mc(xm1, xc0, xp1);
+    R mhL = xm1 - h * un_m1 * sL;
+    R mhR = xc0 - h * un_c0 * sR;
+    R L, Rr;
+    if (ppm) {
+        R lo, hi;
+        ppm_edges(xm2, xm1, xc0, lo, hi);
+        L = hi + mhL - xm1;
+        ppm_edges(xm1, xc0, xp1, lo, hi);
+        Rr = lo + mhR - xc0;
+    } else {
+        L = mhL + R(0.5) * sL;
+        Rr = mhR + R(-0.5) * sR;
+    }
+    return frho >= R(0) ? frho * L : frho * Rr;
+}
+
 template <class R>
 static void step_march1d(const orc_params* p, const orc_step_args* a, const R* uold, R* unew) {
     Grid g(p);
@@ -747,6 +771,29 @@ static void step_march1d(const orc_params* p, const orc_step_args* a, const R* u
                     };
                     F[d][g.idx(i, j, k)] = march_face(P_(-2), P_(-1), P_(0), P_(1), d, P, dtdx, ch, ppm);
                 }
+    // species fractions and their lower-face fluxes
+    const int nsp = p->nsp;
+    std::vector<R> X((size_t)nsp * g.n), FS((size_t)3 * nsp * g.n);
+    for (int s = 0; s < nsp; ++s)
+        for (size_t c = 0; c < g.n; ++c) X[(size_t)s * g.n + c] = uold[(size_t)(9 + s) * g.n + c] / prim[c][0];
+    const R h = R(0.5) * dtdx;
+#pragma omp parallel for num_threads(nthreads()) schedule(static)
+    for (int k = 0; k < g.nz; ++k)
+        for (int j = 0; j < g.ny; ++j)
+            for (int i = 0; i < g.nx; ++i)
+                for (int d = 0; d < 3; ++d) {
+                    int o[3] = {d == 0, d == 1, d == 2};
+                    auto I_ = [&](int s) {
+                        return g.idx(Grid::wr(i + s * o[0], g.nx), Grid::wr(j + s * o[1], g.ny), Grid::wr(k + s * o[2], g.nz));
+                    };
+                    size_t c = g.idx(i, j, k);
+                    for (int s = 0; s < nsp; ++s) {
+                        const R* x = X.data() + (size_t)s * g.n;
+                        FS[((size_t)d * nsp + s) * g.n + c] =
+                            species_face(x[I_(-2)], x[I_(-1)], x[I_(0)], x[I_(1)], prim[I_(-1)][1 + d], prim[I_(0)][1 + d], h,
+                                         F[d][c][0], ppm);
+                    }
+                }
 #pragma omp parallel for num_threads(nthreads()) schedule(static)
     for (int k = 0; k < g.nz; ++k)
         for (int j = 0; j < g.ny; ++j)
@@ -760,6 +807,14 @@ static void step_march1d(const orc_params* p, const orc_step_args* a, const R* u
                     R u = uold[(size_t)v * g.n + c] - dtdx * div;
                     if (v == 8) u = u * glm_fac;
                     unew[(size_t)v * g.n + c] = u;
+                }
+                for (int s = 0; s < nsp; ++s) {
+                    R div = R(0);
+                    for (int d = 0; d < 3; ++d) {
+                        const R* f = FS.data() + ((size_t)d * nsp + s) * g.n;
+                        div = div + (f[cp[d]] - f[c]);
+                    }
+                    unew[(size_t)(9 + s) * g.n + c] = uold[(size_t)(9 + s) * g.n + c] - dtdx * div;
                 }
             }
 }

@@ -35,6 +35,8 @@ typedef struct orc_params {
     double smallp;      /* march/CT pressure floor (spike_mhd.cu:52); GLM uses smallr*smallc^2/gamma */
     double llf_dmin, llf_pmin;
     double turb_min_rho;
+    int32_t nsp;        /* march only: passive species, planes 9..9+nsp-1 hold rho*X */
+    int32_t pad;
 } orc_params;
 
 typedef struct orc_step_args {

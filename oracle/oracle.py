@@ -33,7 +33,7 @@ class OrcParams(C.Structure):
                 ("emf", C.c_int32), ("ct_halfslope", C.c_int32),
                 ("boxlen", C.c_double), ("gamma", C.c_double), ("smallr", C.c_double),
                 ("smallc", C.c_double), ("smallp", C.c_double), ("llf_dmin", C.c_double),
-                ("llf_pmin", C.c_double), ("turb_min_rho", C.c_double)]
+                ("llf_pmin", C.c_double), ("turb_min_rho", C.c_double), ("nsp", C.c_int32), ("pad", C.c_int32)]
 
 
 class OrcStepArgs(C.Structure):
@@ -117,13 +117,14 @@ class Config:
     llf_dmin: float = 0.0
     llf_pmin: float = 0.0
     turb_min_rho: float = 1e-5
+    nsp: int = 0                 # march only: passive species planes after the 9 MHD planes
 
     def c(self) -> OrcParams:
         nx, ny, nz = self.n
         return OrcParams(nx, ny, nz, RECON[self.recon], RIEMANN[self.riemann], int(self.iflo),
                          EMF[self.emf], int(self.ct_halfslope), self.boxlen, self.gamma,
                          self.smallr, self.smallc, self.smallp, self.llf_dmin, self.llf_pmin,
-                         self.turb_min_rho)
+                         self.turb_min_rho, int(self.nsp), 0)
 
     @property
     def dx(self) -> float:

@@ -61,3 +61,22 @@ def test_spinup_reaches_target_mach():
     assert d["finite"] and d["vrms"] / np.sqrt(5 / 3 * 0.6) >= 0.3 and t < 2.0
     E = s.ke_spectrum(u, kmax=8)
     assert E[1:4].sum() > E[5:9].sum() > 0   # energy injected at |k| <= 3 dominates
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_density_pdf_matches_numpy(oracle, dtype):
+    from glmmhdturb_b200 import Solver
+    n = (32, 24, 20)
+    u0 = perturbed_glm_state(oracle, n, seed=6)
+    s = Solver(n, dtype=dtype, gamma=5 / 3)
+    tdt = torch.float64 if dtype == "f64" else torch.float32
+    ud = to_dev(u0, tdt)
+    pdf, st = s.density_pdf(ud, nbins=40, smin=-2.0, smax=2.0)
+    rho = ud[0].double().cpu().numpy()
+    sv = np.log(rho / rho.mean())
+    counts, _ = np.histogram(sv, bins=40, range=(-2.0, 2.0))
+    np.testing.assert_allclose(pdf * rho.size * 0.1, counts, rtol=0, atol=1e-9)
+    assert abs(st["rho_mean"] - rho.mean()) <= 1e-13 * rho.mean()
+    assert abs(st["sigma_s"] - sv.std()) <= 1e-10 * sv.std()
+    again, st2 = s.density_pdf(ud, nbins=40, smin=-2.0, smax=2.0)
+    assert np.array_equal(again, pdf) and st2 == st    # deterministic

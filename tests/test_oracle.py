@@ -174,3 +174,35 @@ def test_oracle_jvp_matches_step_and_finite_differences(oracle):
           O.step_unsplit(cfg, u, dt, smax, fac, ramp=0.4, modes=f.modes * (1 - ea))) / (2 * ea)
     assert np.abs(fa - ja).max() <= 1e-5 * np.abs(ja).max()   # FD roundoff ~1e-16/ea
     assert np.abs(ja[[0, 5, 6, 7, 8]]).max() == 0.0   # the kick moves momentum and energy only
+
+
+def _march_species_state(O, n, nsp, seed):
+    cfg = O.Config(n=(n, n, n), gamma=5 / 3, recon="mc", riemann="hll", nsp=nsp)
+    u = _generic_state(O, n, seed)
+    rng = np.random.default_rng(seed + 100)
+    sp = np.empty((nsp,) + u.shape[1:])
+    for s in range(nsp):
+        sp[s] = u[0] * (0.2 + 0.6 * rng.random(u.shape[1:]))
+    return cfg, np.ascontiguousarray(np.concatenate([u, sp])), u
+
+
+@pytest.mark.parametrize("recon", ["mc", "ppm"])
+def test_march_species_cma_properties(oracle, recon):
+    """Passive species on the march scheme (spike_mhd.cu NSP, CMA): the MHD planes are untouched by
+    the species, sum(rho X) is conserved, and a uniform fraction stays uniform."""
+    O = oracle
+    n = 8
+    cfg, u, u9 = _march_species_state(O, n, 2, 5)
+    cfg.recon = recon
+    cfg9 = O.Config(n=(n, n, n), gamma=5 / 3, recon=recon, riemann="hll")
+    cmax, smax = O.cfl(cfg9, u9)
+    dt = 0.3 * cfg.dx / cmax
+    out = O.step_march1d(cfg, u, dt, smax, 0.98)
+    np.testing.assert_array_equal(out[:9], O.step_march1d(cfg9, u9, dt, smax, 0.98))
+    for s in (9, 10):
+        assert abs(out[s].sum() - u[s].sum()) <= 1e-12 * np.abs(u[s]).sum()
+    # a uniform fraction X = 0.3 stays 0.3
+    u[9] = 0.3 * u[0]
+    out = O.step_march1d(cfg, u, dt, smax, 0.98)
+    X = out[9] / np.maximum(out[0], cfg.smallr)
+    assert np.abs(X - 0.3).max() <= 1e-13
