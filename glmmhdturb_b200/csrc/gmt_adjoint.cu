@@ -12,9 +12,9 @@ template <class R> __global__ void __launch_bounds__(128) adj_faces_kernel(const
     const size_t n = (size_t)A.nx * A.ny * A.nz;
     GMT_ADJ_LOOP adj_faces_cell(A, c);
 }
-template <class R> __global__ void __launch_bounds__(128) adj_flux_kernel(const AdjArgs<R> A) {
+template <int RIEM, class R> __global__ void __launch_bounds__(128) adj_flux_kernel(const AdjArgs<R> A) {
     const size_t n = (size_t)A.nx * A.ny * A.nz;
-    GMT_ADJ_LOOP adj_flux_cell(A, c);
+    GMT_ADJ_LOOP adj_flux_cell<RIEM>(A, c);
 }
 template <class R> __global__ void __launch_bounds__(128) adj_update_kernel(const AdjArgs<R> A) {
     const size_t n = (size_t)A.nx * A.ny * A.nz;
@@ -29,9 +29,9 @@ template <class R> __global__ void __launch_bounds__(128) adj_update_kernel(cons
     }
     if (threadIdx.x == 0 && A.damp) atomicAdd(A.damp, red[0]);
 }
-template <class R> __global__ void __launch_bounds__(128) adj_riemann_kernel(const AdjArgs<R> A) {
+template <int RIEM, class R> __global__ void __launch_bounds__(128) adj_riemann_kernel(const AdjArgs<R> A) {
     const size_t n = (size_t)A.nx * A.ny * A.nz;
-    GMT_ADJ_LOOP adj_riemann_cell(A, c);
+    GMT_ADJ_LOOP adj_riemann_cell<RIEM>(A, c);
 }
 template <class R> __global__ void __launch_bounds__(128) adj_recon_kernel(const AdjArgs<R> A) {
     const size_t n = (size_t)A.nx * A.ny * A.nz;
@@ -48,9 +48,13 @@ template <class R> cudaError_t launch_adjoint(const AdjArgs<R>& A, cudaStream_t 
     const size_t n = (size_t)A.nx * A.ny * A.nz;
     const int nb = (int)std::min<size_t>((n + 127) / 128, 148 * 16);
     adj_faces_kernel<R><<<nb, 128, 0, s>>>(A);
-    adj_flux_kernel<R><<<nb, 128, 0, s>>>(A);
+    if (A.riem == RIEM_HLL) adj_flux_kernel<RIEM_HLL, R><<<nb, 128, 0, s>>>(A);
+    else if (A.riem == RIEM_LLF_BOUND) adj_flux_kernel<RIEM_LLF_BOUND, R><<<nb, 128, 0, s>>>(A);
+    else adj_flux_kernel<RIEM_HLLD, R><<<nb, 128, 0, s>>>(A);
     adj_update_kernel<R><<<nb, 128, 0, s>>>(A);
-    adj_riemann_kernel<R><<<nb, 128, 0, s>>>(A);
+    if (A.riem == RIEM_HLL) adj_riemann_kernel<RIEM_HLL, R><<<nb, 128, 0, s>>>(A);
+    else if (A.riem == RIEM_LLF_BOUND) adj_riemann_kernel<RIEM_LLF_BOUND, R><<<nb, 128, 0, s>>>(A);
+    else adj_riemann_kernel<RIEM_HLLD, R><<<nb, 128, 0, s>>>(A);
     adj_recon_kernel<R><<<nb, 128, 0, s>>>(A);
     adj_gather_kernel<R><<<nb, 128, 0, s>>>(A);
     return cudaGetLastError();

@@ -142,50 +142,78 @@ template <class R> GMT_HD void slope_deriv(R dl, R dr, bool mm, R& gl, R& gr) {
     }
 }
 
-template <int D, class R>
-GMT_HD Q9<R> riemann_any(const Q9<R>& L, const Q9<R>& Rr, const Consts<R>& K, R ch, bool use_llf,
-                                             int riem) {
-    if (riem == RIEM_HLL) return riemann_glm<D, RIEM_HLL>(L, Rr, K, ch, use_llf);
-    if (riem == RIEM_LLF_BOUND) return riemann_glm<D, RIEM_LLF_BOUND>(L, Rr, K, ch, use_llf);
-    return riemann_glm<D, RIEM_HLLD>(L, Rr, K, ch, use_llf);
+// the cyclic rotation that makes direction d the x normal, and its inverse, for a runtime d
+// (rot_to / rot_from of the physics, glmmhd_turb.jl:118-138): a Jacobian evaluated in the x
+// frame serves all three directions, J_d^T v = rot_from_d(J_x^T rot_to_d(v))
+template <class R> GMT_HD Q9<R> rot_to_d(const Q9<R>& q, int d) {
+    if (d == 0) return q;
+    Q9<R> r;
+    if (d == 1) {
+        r.v[0] = q.v[0]; r.v[1] = q.v[2]; r.v[2] = q.v[3]; r.v[3] = q.v[1]; r.v[4] = q.v[4];
+        r.v[5] = q.v[6]; r.v[6] = q.v[7]; r.v[7] = q.v[5]; r.v[8] = q.v[8];
+    } else {
+        r.v[0] = q.v[0]; r.v[1] = q.v[3]; r.v[2] = q.v[1]; r.v[3] = q.v[2]; r.v[4] = q.v[4];
+        r.v[5] = q.v[7]; r.v[6] = q.v[5]; r.v[7] = q.v[6]; r.v[8] = q.v[8];
+    }
+    return r;
+}
+template <class R> GMT_HD Q9<R> rot_from_d(const Q9<R>& f, int d) {
+    if (d == 0) return f;
+    Q9<R> r;
+    if (d == 1) {
+        r.v[0] = f.v[0]; r.v[1] = f.v[3]; r.v[2] = f.v[1]; r.v[3] = f.v[2]; r.v[4] = f.v[4];
+        r.v[5] = f.v[7]; r.v[6] = f.v[5]; r.v[7] = f.v[6]; r.v[8] = f.v[8];
+    } else {
+        r.v[0] = f.v[0]; r.v[1] = f.v[2]; r.v[2] = f.v[3]; r.v[3] = f.v[1]; r.v[4] = f.v[4];
+        r.v[5] = f.v[6]; r.v[6] = f.v[7]; r.v[7] = f.v[5]; r.v[8] = f.v[8];
+    }
+    return r;
 }
 
-// Lbar, Rbar = J^T Fbar of the Riemann solve at a D face (18 inputs in chunks of NCH)
-template <int D, class R>
-GMT_HD void riemann_adj(const Q9<R>& L, const Q9<R>& Rr, const Q9<R>& Fb, const Consts<R>& K, R ch,
-                                            bool use_llf, int riem, Q9<R>& Lb, Q9<R>& Rb) {
+// the flux at a face of direction d: riemann_glm<d> = rot_from_d . riemann_glm<0> . rot_to_d
+template <int RIEM, class R>
+GMT_HD Q9<R> riemann_dir(const Q9<R>& L, const Q9<R>& Rr, int d, const Consts<R>& K, R ch, bool use_llf) {
+    return rot_from_d(riemann_glm<0, RIEM>(rot_to_d(L, d), rot_to_d(Rr, d), K, ch, use_llf), d);
+}
+
+// Lbar, Rbar = J^T Fbar of the Riemann solve at a face of direction d (18 inputs in chunks of NCH,
+// evaluated in the x frame)
+template <int RIEM, class R>
+GMT_HD void riemann_adj(const Q9<R>& L, const Q9<R>& Rr, const Q9<R>& Fb, int d, const Consts<R>& K, R ch,
+                        bool use_llf, Q9<R>& Lb, Q9<R>& Rb) {
     using DD = Dual<R, NCH>;
     const Consts<DD> KD = dual_consts<R, NCH>(K);
-    Lb = q9_zero<R>();
-    Rb = q9_zero<R>();
+    const Q9<R> Lx = rot_to_d(L, d), Rx = rot_to_d(Rr, d), Fbx = rot_to_d(Fb, d);
+    Q9<R> Lbx = q9_zero<R>(), Rbx = q9_zero<R>();
 #pragma unroll 1
     for (int c0 = 0; c0 < 18; c0 += NCH) {
         Q9<DD> Ld, Rd;
 #pragma unroll
         for (int v = 0; v < 9; ++v) {
-            Ld.v[v] = DD(L.v[v]);
-            Rd.v[v] = DD(Rr.v[v]);
+            Ld.v[v] = DD(Lx.v[v]);
+            Rd.v[v] = DD(Rx.v[v]);
 #pragma unroll
             for (int j = 0; j < NCH; ++j) {
                 Ld.v[v].d[j] = (c0 + j == v) ? R(1) : R(0);
                 Rd.v[v].d[j] = (c0 + j == 9 + v) ? R(1) : R(0);
             }
         }
-        Q9<DD> F = riemann_any<D>(Ld, Rd, KD, DD(ch), use_llf, riem);
+        Q9<DD> F = riemann_glm<0, RIEM>(Ld, Rd, KD, DD(ch), use_llf);
 #pragma unroll
         for (int j = 0; j < NCH; ++j) {
             R acc = R(0);
 #pragma unroll
-            for (int v = 0; v < 9; ++v) acc += Fb.v[v] * F.v[v].d[j];
+            for (int v = 0; v < 9; ++v) acc += Fbx.v[v] * F.v[v].d[j];
 #pragma unroll
             for (int v = 0; v < 9; ++v) {
-                if (c0 + j == v) Lb.v[v] = acc;
-                if (c0 + j == 9 + v) Rb.v[v] = acc;
+                if (c0 + j == v) Lbx.v[v] = acc;
+                if (c0 + j == 9 + v) Rbx.v[v] = acc;
             }
         }
     }
+    Lb = rot_from_d(Lbx, d);
+    Rb = rot_from_d(Rbx, d);
 }
-
 
 template <class R> GMT_HD void cell_xyz(const AdjArgs<R>& A, size_t c, int& x, int& y, int& z) {
     x = (int)(c % A.nx);
@@ -202,14 +230,9 @@ template <class R> GMT_HD Q9<R> fs_get(const R* FS, size_t n, size_t c, int k) {
     return q;
 }
 
-template <class R> struct FluxFn {
+template <class R> struct FluxXFn {   // the x-normal ideal MHD flux
     R gamma;
-    int d;
-    template <class T> GMT_HD Q9<T> operator()(const Q9<T>& q) const {
-        if (d == 0) return dir_flux<0>(q, T(gamma));
-        if (d == 1) return dir_flux<1>(q, T(gamma));
-        return dir_flux<2>(q, T(gamma));
-    }
+    template <class T> GMT_HD Q9<T> operator()(const Q9<T>& q) const { return phys_flux_x(q, T(gamma)); }
 };
 template <class R> struct C2PFn {
     Consts<R> K;
@@ -239,20 +262,18 @@ template <class R> GMT_HD void adj_faces_cell(const AdjArgs<R>& A, size_t c) {
 }
 
 // pass 2: the fluxes at the +x, +y, +z faces of cell c
-template <class R> GMT_HD void adj_flux_cell(const AdjArgs<R>& A, size_t c) {
+template <int RIEM, class R> GMT_HD void adj_flux_cell(const AdjArgs<R>& A, size_t c) {
     const Idx<R> I = idx_of(A);
     const bool ul = A.use_llf != 0;
     int x, y, z;
     cell_xyz(A, c, x, y, z);
-    Q9<R> F0 = riemann_any<0>(fs_get(A.FS, I.n, c, 0), fs_get(A.FS, I.n, I.at(x + 1, y, z), 1), A.K, A.ch, ul, A.riem);
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+        const size_t cp = d == 0 ? I.at(x + 1, y, z) : (d == 1 ? I.at(x, y + 1, z) : I.at(x, y, z + 1));
+        const Q9<R> F = riemann_dir<RIEM>(fs_get(A.FS, I.n, c, 2 * d), fs_get(A.FS, I.n, cp, 2 * d + 1), d, A.K, A.ch, ul);
 #pragma unroll
-    for (int v = 0; v < 9; ++v) A.FL[(size_t)v * I.n + c] = F0.v[v];
-    Q9<R> F1 = riemann_any<1>(fs_get(A.FS, I.n, c, 2), fs_get(A.FS, I.n, I.at(x, y + 1, z), 3), A.K, A.ch, ul, A.riem);
-#pragma unroll
-    for (int v = 0; v < 9; ++v) A.FL[(size_t)(9 + v) * I.n + c] = F1.v[v];
-    Q9<R> F2 = riemann_any<2>(fs_get(A.FS, I.n, c, 4), fs_get(A.FS, I.n, I.at(x, y, z + 1), 5), A.K, A.ch, ul, A.riem);
-#pragma unroll
-    for (int v = 0; v < 9; ++v) A.FL[(size_t)(18 + v) * I.n + c] = F2.v[v];
+        for (int v = 0; v < 9; ++v) A.FL[(size_t)(9 * d + v) * I.n + c] = F.v[v];
+    }
 }
 
 // pass 3: the update and its epilogue; returns this cell's part of dL/d(amplitude)
@@ -316,7 +337,7 @@ template <class R> GMT_HD double adj_update_cell(const AdjArgs<R>& A, size_t c) 
 }
 
 // pass 4: adjoint of the Riemann solves at the +x, +y, +z faces of cell c
-template <class R> GMT_HD void adj_riemann_cell(const AdjArgs<R>& A, size_t c) {
+template <int RIEM, class R> GMT_HD void adj_riemann_cell(const AdjArgs<R>& A, size_t c) {
     const Idx<R> I = idx_of(A);
     const bool ul = A.use_llf != 0;
     int x, y, z;
@@ -328,9 +349,7 @@ template <class R> GMT_HD void adj_riemann_cell(const AdjArgs<R>& A, size_t c) {
 #pragma unroll
         for (int v = 0; v < 9; ++v) Fb.v[v] = A.dtdx * (A.R1b[(size_t)v * I.n + cp] - A.R1b[(size_t)v * I.n + c]);
         const Q9<R> L = fs_get(A.FS, I.n, c, 2 * d), Rr = fs_get(A.FS, I.n, cp, 2 * d + 1);
-        if (d == 0) riemann_adj<0>(L, Rr, Fb, A.K, A.ch, ul, A.riem, Lb, Rb);
-        else if (d == 1) riemann_adj<1>(L, Rr, Fb, A.K, A.ch, ul, A.riem, Lb, Rb);
-        else riemann_adj<2>(L, Rr, Fb, A.K, A.ch, ul, A.riem, Lb, Rb);
+        riemann_adj<RIEM>(L, Rr, Fb, d, A.K, A.ch, ul, Lb, Rb);
 #pragma unroll
         for (int v = 0; v < 9; ++v) {
             A.FSb[(size_t)((2 * d) * 9 + v) * I.n + c] = Lb.v[v];
@@ -375,8 +394,10 @@ template <class R> GMT_HD void adj_recon_cell(const AdjArgs<R>& A, size_t c) {
         for (int v = 0; v < 9; ++v) Fb.v[v] = -h * uhb.v[v];
 #pragma unroll 1
         for (int d = 0; d < 3; ++d) {
-            const Q9<R> jp = vjp9<3>(FluxFn<R>{A.K.gamma, d}, padd(r.m0, r.s[d], R(1)), Fb);
-            const Q9<R> jm = vjp9<3>(FluxFn<R>{A.K.gamma, d}, padd(r.m0, r.s[d], R(-1)), Fb);
+            // dir_flux<d> = rot_from_d . phys_flux_x . rot_to_d
+            const Q9<R> Fbx = rot_to_d(Fb, d);
+            const Q9<R> jp = rot_from_d(vjp9<3>(FluxXFn<R>{A.K.gamma}, rot_to_d(padd(r.m0, r.s[d], R(1)), d), Fbx), d);
+            const Q9<R> jm = rot_from_d(vjp9<3>(FluxXFn<R>{A.K.gamma}, rot_to_d(padd(r.m0, r.s[d], R(-1)), d), Fbx), d);
 #pragma unroll
             for (int v = 0; v < 9; ++v) {
                 m0b.v[v] += jp.v[v] - jm.v[v];
