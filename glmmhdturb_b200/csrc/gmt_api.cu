@@ -111,13 +111,20 @@ template <class R> Consts<R> consts_of(const gmt_params& p) {
 
 int choose_tile(gmt_ctx* c) {
     const gmt_params& p = c->p;
-    static const int cand[][2] = {{32, 8}, {32, 4}, {16, 8}, {16, 4}, {8, 8}, {8, 4}, {4, 4}, {8, 2},
-                                  {4, 2}, {2, 2}, {8, 1}, {4, 1}, {2, 1}, {1, 1}};
+    // largest first: 32x16 (512 threads, one block per SM) measured fastest at 512^3 FP32 for
+    // both the unsplit and the march scheme; FP64 stops at 256 threads
+    static const int cand[][2] = {{32, 16}, {32, 8}, {32, 4}, {16, 8}, {16, 4}, {8, 8}, {8, 4}, {4, 4},
+                                  {8, 2}, {4, 2}, {2, 2}, {8, 1}, {4, 1}, {2, 1}, {1, 1}};
     int ox = p.tile_x, oy = p.tile_y;
     if (ox <= 0 || oy <= 0) {
         ox = oy = 0;
         for (auto& t : cand)
-            if (divides(p.nx, t[0]) && divides(p.ny, t[1])) { ox = t[0]; oy = t[1]; break; }
+            if (divides(p.nx, t[0]) && divides(p.ny, t[1]) && t[0] * t[1] <= unsplit_max_threads(c->esize) &&
+                unsplit_smem(c->esize, t[0], t[1]) <= 227 * 1024) {
+                ox = t[0];
+                oy = t[1];
+                break;
+            }
     }
     if (!divides(p.nx, ox) || !divides(p.ny, oy))
         return fail(GMT_ERR_ARG, "tile " + std::to_string(ox) + "x" + std::to_string(oy) + " does not divide the grid");
@@ -177,7 +184,33 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         if (e != cudaSuccess) return cuda_fail(e, "unsplit step");
         return GMT_OK;
     }
+    if (p.scheme == GMT_SCHEME_MARCH1D && p.nsp == 0) {
+        // the tiled march: the unsplit tile with the march scheme (one solve per face)
+        UnsplitArgs<R> A;
+        A.u = u; A.o = o;
+        A.nx = p.nx; A.ny = p.ny; A.nz = p.nz;
+        A.ox = c->ox; A.oy = c->oy; A.lz = c->lz;
+        A.dt = (R)a->dt; A.dtdx = (R)(a->dt / dx);
+        A.ch = (R)a->ch; A.glm_fac = (R)a->glm_fac;
+        A.ramp = R(1);
+        A.K = consts_of<R>(p);
+        A.iflo = 0; A.use_llf = 0; A.do_turb = 0;
+        A.btab = nullptr;
+        A.trigx = static_cast<const R*>(c->trig[0]);
+        A.cfl_out = nullptr;
+        A.err = c->err;
+        A.dx = (R)dx;
+        A.dparams = nullptr;
+        if (a->want_cfl) {
+            GMT_CUDA(cudaMemsetAsync(c->cfl, 0, 2 * sizeof(unsigned long long), s));
+            A.cfl_out = c->cfl;
+        }
+        cudaError_t e = launch_march_tiled(A, p.recon, s);
+        if (e != cudaSuccess) return cuda_fail(e, "march step");
+        return GMT_OK;
+    }
     if (p.scheme == GMT_SCHEME_MARCH1D) {
+        // with passive species: one thread per cell
         MarchArgs<R> A;
         A.u = u; A.o = o;
         A.nx = p.nx; A.ny = p.ny; A.nz = p.nz;
@@ -325,7 +358,7 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     c->n = (size_t)p->nx * p->ny * p->nz;
     cudaGetDevice(&c->device);
     int rc = GMT_OK;
-    if (p->scheme == GMT_SCHEME_UNSPLIT) rc = choose_tile(c);
+    if (p->scheme == GMT_SCHEME_UNSPLIT || (p->scheme == GMT_SCHEME_MARCH1D && p->nsp == 0)) rc = choose_tile(c);
     if (rc != GMT_OK) { delete c; return rc; }
     auto alloc = [&](void** ptr, size_t bytes) -> bool {
         cudaError_t e = cudaMalloc(ptr, bytes);
@@ -418,7 +451,13 @@ int gmt_kernel_info(gmt_ctx* c, int32_t* regs, int64_t* smem, int32_t tile[3]) {
                          c->ox * c->oy);
         sm = (int64_t)unsplit_smem(c->esize, c->ox, c->oy);
     } else if (c->p.scheme == GMT_SCHEME_MARCH1D) {
-        r = march1d_regs(c->esize);
+        if (c->p.nsp > 0) {
+            r = march1d_regs(c->esize);
+        } else {
+            r = c->esize == 8 ? march_tiled_regs((const UnsplitArgs<double>*)nullptr, c->p.recon, c->ox * c->oy)
+                              : march_tiled_regs((const UnsplitArgs<float>*)nullptr, c->p.recon, c->ox * c->oy);
+            sm = (int64_t)unsplit_smem(c->esize, c->ox, c->oy);
+        }
     } else {
         r = ct_regs_of(c->esize);
         sm = (int64_t)ct_smem_of(c->esize, c->ox, c->oy);

@@ -23,6 +23,11 @@ cudaError_t launch_ensemble(const UnsplitArgs<float>* boxes, const EnsItem* item
 cudaError_t launch_ensemble(const UnsplitArgs<double>* boxes, const EnsItem* items, int nitems, unsigned* queue,
                             int recon, int riem, int nsm, cudaStream_t s);
 size_t unsplit_smem(int dtype_bytes, int ox, int oy);
+// tiled march (the unsplit tile with the march scheme; no passive species)
+cudaError_t launch_march_tiled(const UnsplitArgs<float>& A, int recon, cudaStream_t s);
+cudaError_t launch_march_tiled(const UnsplitArgs<double>& A, int recon, cudaStream_t s);
+int march_tiled_regs(const UnsplitArgs<float>*, int recon, int nthreads);
+int march_tiled_regs(const UnsplitArgs<double>*, int recon, int nthreads);
 int unsplit_regs(int dtype_bytes, int recon, int riem, int nthreads);
 
 // transverse-free 1-D Hancock march (gmt_march1d.cu)

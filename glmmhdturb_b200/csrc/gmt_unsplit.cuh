@@ -114,12 +114,12 @@ __device__ __forceinline__ void stage_plane(R* __restrict__ SG, const CPlanes<R>
 
 template <class R>
 __device__ __forceinline__ void unstage_plane(R* __restrict__ PRs, const R* __restrict__ SG, int PN, const Consts<R>& K,
-                                              int tid, int nt) {
+                                              R pfloor, int tid, int nt) {
     for (int c = tid; c < PN; c += nt) {
         Q9<R> q;
 #pragma unroll
         for (int v = 0; v < 9; ++v) q.v[v] = SG[v * PN + c];
-        q = cons2prim(q, K.gamma, K.smallr, K.pfl);
+        q = cons2prim(q, K.gamma, K.smallr, pfloor);
 #pragma unroll
         for (int v = 0; v < 9; ++v) PRs[v * PN + c] = q.v[v];
     }
@@ -130,12 +130,111 @@ template <class R> __host__ __device__ inline size_t unsplit_smem_bytes(int ox, 
     return (27 * PN + 36 * RN + 9 * PN) * sizeof(R) + 40 * sizeof(double);
 }
 
+// The two schemes that share the tile march.  A scheme supplies the primitive floor of the
+// staged planes, the reconstruction of a cell (recon, then prep<D> before the states of
+// direction D), its interface states, the face flux and the update epilogue.
+//
+// Unsplit (integrator_tiled!/plm!/plm_ppm!): one MUSCL-Hancock predictor over all three
+// directions, iflo revert, HLLD/HLL/LLF + GLM, void floor, psi damping and forcing kick.
+template <class R, int RECON, int RIEM> struct UnsplitScheme {
+    using Cell = Rec<R>;
+    static __device__ __forceinline__ R prim_floor(const Consts<R>& K) { return K.pfl; }
+    static __device__ __forceinline__ void recon(const R* PR, int PN, int PW, int c, int s0, int sm, int sp,
+                                                 const Consts<R>& K, R dtdx, Cell& r) {
+        recon_prims<R, RECON>(PR, PN, PW, c, s0, sm, sp, K, dtdx, r);
+    }
+    template <int D>
+    static __device__ __forceinline__ void prep(Cell&, const R*, int, int, int, int, int, int, const Consts<R>&, R) {}
+    template <int D, int SIGN>
+    static __device__ __forceinline__ Q9<R> state(const Cell& r, const R* PR, int PN, int PW, int c, int s0, int sm,
+                                                  int sp, const Consts<R>& K, int iflo) {
+        return face_state<R, RECON, D, SIGN>(r, PR, PN, PW, c, s0, sm, sp, K, iflo);
+    }
+    template <int D>
+    static __device__ __forceinline__ Q9<R> flux(const Q9<R>& L, const Q9<R>& Rr, const Consts<R>& K, R ch, bool llf) {
+        return riemann_glm<D, RIEM>(L, Rr, K, ch, llf);
+    }
+    static __device__ __forceinline__ void finish(Q9<R>& q, const Consts<R>& K, R glm_fac, bool turb, R ax, R ay, R az,
+                                                  R dt) {
+        finish_update(q, K, glm_fac, turb, ax, ay, az, dt);
+    }
+};
+
+// March (spike_mhd.cu:65-223, 257-299): per direction a full MonCen slope and a transverse-free
+// 1-D Hancock half step of the cell, faces at mh -+ s/2 (or the Julia-form PPM edge plus the
+// predictor shift), floors rho >= smallr and p >= smallp, HLL with GLM cleaning; the update is
+// u - dt/dx sum_d (F_hi - F_lo) and psi *= glm_fac.  The unsplit tile's update
+// u + dt/dx ((F_xlo - F_xhi) + (F_ylo - F_yhi) + (F_zlo - F_zhi)) is the same IEEE value, since
+// negation is exact and round-to-nearest is sign-symmetric.
+template <class R> struct MarchCell {
+    Q9<R> m0, s, mh;   // cell primitives; slope and 1-D predictor of the direction being prepared
+};
+template <class R, int RECON> struct MarchScheme {
+    using Cell = MarchCell<R>;
+    static __device__ __forceinline__ R prim_floor(const Consts<R>& K) { return K.smallp; }
+    static __device__ __forceinline__ void recon(const R* PR, int PN, int, int c, int s0, int, int, const Consts<R>&, R,
+                                                 Cell& r) {
+        const R* P0 = PR + (size_t)s0 * 9 * PN;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) r.m0.v[v] = P0[v * PN + c];
+    }
+    template <int D>
+    static __device__ __forceinline__ void neighbours(const R* PR, int PN, int PW, int c, int s0, int sm, int sp,
+                                                      Q9<R>& L, Q9<R>& Rr) {
+        const R* PL = PR + (size_t)(D == 2 ? sm : s0) * 9 * PN;
+        const R* PP = PR + (size_t)(D == 2 ? sp : s0) * 9 * PN;
+        const int cl = D == 0 ? c - 1 : (D == 1 ? c - PW : c), cr = D == 0 ? c + 1 : (D == 1 ? c + PW : c);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) { L.v[v] = PL[v * PN + cl]; Rr.v[v] = PP[v * PN + cr]; }
+    }
+    template <int D>
+    static __device__ __forceinline__ void prep(Cell& r, const R* PR, int PN, int PW, int c, int s0, int sm, int sp,
+                                                const Consts<R>& K, R dtdx) {
+        Q9<R> L, Rr;
+        neighbours<D>(PR, PN, PW, c, s0, sm, sp, L, Rr);
+        r.s = full_slope(L, r.m0, Rr);
+        r.mh = hanc1d<D>(r.m0, r.s, dtdx, K.gamma, K.smallr, K.smallp);
+    }
+    template <int D, int SIGN>
+    static __device__ __forceinline__ Q9<R> state(const Cell& r, const R* PR, int PN, int PW, int c, int s0, int sm,
+                                                  int sp, const Consts<R>& K, int) {
+        Q9<R> f;
+        if (RECON == RECON_PPM) {
+            Q9<R> L, Rr;
+            neighbours<D>(PR, PN, PW, c, s0, sm, sp, L, Rr);
+#pragma unroll
+            for (int v = 0; v < 9; ++v) {
+                R lo, hi;
+                ppm_edges(L.v[v], r.m0.v[v], Rr.v[v], lo, hi);
+                f.v[v] = (SIGN > 0 ? hi : lo) + r.mh.v[v] - r.m0.v[v];
+            }
+        } else {
+            f = padd(r.mh, r.s, SIGN > 0 ? R(0.5) : R(-0.5));
+        }
+        f.v[0] = rmax(f.v[0], K.smallr);
+        f.v[4] = rmax(f.v[4], K.smallp);
+        return f;
+    }
+    template <int D>
+    static __device__ __forceinline__ Q9<R> flux(const Q9<R>& L, const Q9<R>& Rr, const Consts<R>& K, R ch, bool) {
+        Q9<R> Lr = rot_to<D>(L), Rrr = rot_to<D>(Rr);
+        R bns, psis;
+        glm_pair(Lr.v[5], Rrr.v[5], Lr.v[8], Rrr.v[8], ch, bns, psis);
+        Lr.v[5] = bns;
+        Rrr.v[5] = bns;
+        return rot_from<D>(hll_x(Lr, Rrr, K.gamma, bns, psis, ch * ch * bns));
+    }
+    static __device__ __forceinline__ void finish(Q9<R>& q, const Consts<R>&, R glm_fac, bool, R, R, R, R) {
+        q.v[8] = q.v[8] * glm_fac;
+    }
+};
+
 // One tile (bx, by) x z-chunk bz of one box.  TOX, TOY > 0 fix the tile at compile time
 // (constant shared-memory offsets); 0 = runtime tile.  Used by the single-box kernel (one tile per
 // block) and by the ensemble kernel (a queue of tiles over many boxes).
-template <class R, int RECON, int RIEM, int TOX, int TOY>
-__device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const StepVals<R>& V, int bx, int by, int bz,
-                                             unsigned char* smem_raw) {
+template <class R, class S, int TOX, int TOY>
+__device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepVals<R>& V, int bx, int by, int bz,
+                                            unsigned char* smem_raw) {
     const int OX = TOX > 0 ? TOX : A.ox, OY = TOY > 0 ? TOY : A.oy;
     const int PW = OX + 4, PN = (OX + 4) * (OY + 4);
     const int RW = OX + 2, RN = (OX + 2) * (OY + 2);
@@ -160,7 +259,7 @@ __device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const Step
         stage_plane(SG, A.u, PN, PW, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
         cp_async_wait_all();
         __syncthreads();
-        unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, SG, PN, K, tid, NT);
+        unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, SG, PN, K, S::prim_floor(K), tid, NT);
         if (j == 2 && tid == 0) mbar_init(mbar, NT);
         __syncthreads();
     }
@@ -197,18 +296,21 @@ __device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const Step
                 for (int v = 0; v < 9; ++v)
                     XY.v[v] = (ST[(1 * 9 + v) * RN + rown] - Fxh.v[v]) + (ST[(3 * 9 + v) * RN + rown] - Fyh.v[v]);
             }
-            Rec<R> r;
-            recon_prims<R, RECON>(PR, PN, PW, cown, s0, sm, sp, K, dtdx, r);
+            typename S::Cell r;
+            S::recon(PR, PN, PW, cown, s0, sm, sp, K, dtdx, r);
             if (!first && !last) {
-                st_put(ST + 0 * 9 * RN, RN, rown, face_state<R, RECON, 0, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
-                st_put(ST + 1 * 9 * RN, RN, rown, face_state<R, RECON, 0, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
-                st_put(ST + 2 * 9 * RN, RN, rown, face_state<R, RECON, 1, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
-                st_put(ST + 3 * 9 * RN, RN, rown, face_state<R, RECON, 1, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+                S::template prep<0>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx);
+                st_put(ST + 0 * 9 * RN, RN, rown, S::template state<0, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+                st_put(ST + 1 * 9 * RN, RN, rown, S::template state<0, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+                S::template prep<1>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx);
+                st_put(ST + 2 * 9 * RN, RN, rown, S::template state<1, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+                st_put(ST + 3 * 9 * RN, RN, rown, S::template state<1, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
             }
-            Q9<R> Pz = face_state<R, RECON, 2, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+            S::template prep<2>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx);
+            Q9<R> Pz = S::template state<2, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
             if (!first) {
-                Q9<R> Mz = face_state<R, RECON, 2, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
-                Q9<R> Fzhi = riemann_glm<2, RIEM>(pPz, Mz, K, ch, A.use_llf != 0);
+                Q9<R> Mz = S::template state<2, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+                Q9<R> Fzhi = S::template flux<2>(pPz, Mz, K, ch, A.use_llf != 0);
                 if (kr - 1 >= z0) {
                     const int kf = kr - 1;
                     const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * kf);
@@ -217,7 +319,7 @@ __device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const Step
                     for (int v = 0; v < 9; ++v) q.v[v] = A.u.p[v][g] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
                     R ax = R(0), ay = R(0), az = R(0);
                     if (turb) force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
-                    finish_update(q, K, V.glm_fac, turb, ax, ay, az, V.dt);
+                    S::finish(q, K, V.glm_fac, turb, ax, ay, az, V.dt);
 #pragma unroll
                     for (int v = 0; v < 9; ++v) A.o.p[v][g] = q.v[v];
                     if (A.cfl_out) {
@@ -239,13 +341,18 @@ __device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const Step
                 else if (h < 2 * OY) { int f = h - OY; rc = (OX + 1) + RW * (f + 1); cc = (OX + 2) + PW * (f + 2); which = 1; }
                 else if (h < 2 * OY + OX) { int f = h - 2 * OY; rc = (f + 1); cc = (f + 2) + PW * 1; which = 2; }
                 else { int f = h - 2 * OY - OX; rc = (f + 1) + RW * (OY + 1); cc = (f + 2) + PW * (OY + 2); which = 3; }
-                Rec<R> r;
-                recon_prims<R, RECON>(PR, PN, PW, cc, s0, sm, sp, K, dtdx, r);
+                typename S::Cell r;
+                S::recon(PR, PN, PW, cc, s0, sm, sp, K, dtdx, r);
                 Q9<R> f;
-                if (which == 0) f = face_state<R, RECON, 0, +1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
-                else if (which == 1) f = face_state<R, RECON, 0, -1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
-                else if (which == 2) f = face_state<R, RECON, 1, +1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
-                else f = face_state<R, RECON, 1, -1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
+                if (which < 2) {
+                    S::template prep<0>(r, PR, PN, PW, cc, s0, sm, sp, K, dtdx);
+                    if (which == 0) f = S::template state<0, +1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
+                    else f = S::template state<0, -1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
+                } else {
+                    S::template prep<1>(r, PR, PN, PW, cc, s0, sm, sp, K, dtdx);
+                    if (which == 2) f = S::template state<1, +1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
+                    else f = S::template state<1, -1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
+                }
                 st_put(ST + which * 9 * RN, RN, rc, f);
             }
         }
@@ -253,24 +360,24 @@ __device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const Step
         if (!first && !last) {
             // own faces at x+1/2 and y+1/2: flux kept in registers and written over the right state,
             // where the neighbour reads it as its lower-face flux
-            Fxh = riemann_glm<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, rown), st_get(ST + 1 * 9 * RN, RN, ixh), K, ch,
-                                       A.use_llf != 0);
+            Fxh = S::template flux<0>(st_get(ST + 0 * 9 * RN, RN, rown), st_get(ST + 1 * 9 * RN, RN, ixh), K, ch,
+                                      A.use_llf != 0);
             st_put(ST + 1 * 9 * RN, RN, ixh, Fxh);
-            Fyh = riemann_glm<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, rown), st_get(ST + 3 * 9 * RN, RN, iyh), K, ch,
-                                       A.use_llf != 0);
+            Fyh = S::template flux<1>(st_get(ST + 2 * 9 * RN, RN, rown), st_get(ST + 3 * 9 * RN, RN, iyh), K, ch,
+                                      A.use_llf != 0);
             st_put(ST + 3 * 9 * RN, RN, iyh, Fyh);
             for (int h = NT - 1 - tid; h < OX + OY; h += NT) {
                 // boundary faces on the low x and low y side of the tile, taken by the last threads
                 if (h < OY) {
                     const int il = 0 + RW * (h + 1), ir = 1 + RW * (h + 1);
-                    Q9<R> F = riemann_glm<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, il), st_get(ST + 1 * 9 * RN, RN, ir), K,
-                                                   ch, A.use_llf != 0);
+                    Q9<R> F = S::template flux<0>(st_get(ST + 0 * 9 * RN, RN, il), st_get(ST + 1 * 9 * RN, RN, ir), K,
+                                                  ch, A.use_llf != 0);
                     st_put(ST + 1 * 9 * RN, RN, ir, F);
                 } else {
                     const int c = h - OY;
                     const int il = (c + 1), ir = (c + 1) + RW;
-                    Q9<R> F = riemann_glm<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, il), st_get(ST + 3 * 9 * RN, RN, ir), K,
-                                                   ch, A.use_llf != 0);
+                    Q9<R> F = S::template flux<1>(st_get(ST + 2 * 9 * RN, RN, il), st_get(ST + 3 * 9 * RN, RN, ir), K,
+                                                  ch, A.use_llf != 0);
                     st_put(ST + 3 * 9 * RN, RN, ir, F);
                 }
             }
@@ -278,7 +385,7 @@ __device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const Step
         if (load) {
             mbar_wait(mbar, phase, A.err);
             phase ^= 1u;
-            unstage_plane(PR + mod3(kr + 2) * 9 * PN, SG, PN, K, tid, NT);
+            unstage_plane(PR + mod3(kr + 2) * 9 * PN, SG, PN, K, S::prim_floor(K), tid, NT);
         }
         __syncthreads();
     }
@@ -288,6 +395,12 @@ __device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const Step
         __syncthreads();
         block_max_atomic(smax, A.cfl_out + 1, red);
     }
+}
+
+template <class R, int RECON, int RIEM, int TOX, int TOY>
+__device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const StepVals<R>& V, int bx, int by, int bz,
+                                             unsigned char* smem_raw) {
+    scheme_tile<R, UnsplitScheme<R, RECON, RIEM>, TOX, TOY>(A, V, bx, by, bz, smem_raw);
 }
 
 // A tile = (box, bx, by, bz) work item of the ensemble kernel.
@@ -318,6 +431,13 @@ template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY
 __global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsplit_tile<R, RECON, RIEM, TOX, TOY>(A, step_vals(A), blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
+// Tiled march step (the scheme behind march_run_dev); RECON is RECON_MC or RECON_PPM.
+template <class R, int RECON, int MAXT, int MINB, int TOX = 0, int TOY = 0>
+__global__ void __launch_bounds__(MAXT, MINB) march_tile_kernel(const UnsplitArgs<R> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    scheme_tile<R, MarchScheme<R, RECON>, TOX, TOY>(A, step_vals(A), blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 }  // namespace gmt

@@ -1,4 +1,4 @@
-// FP32 unsplit step kernels, built with --use_fast_math (approximate reciprocal and square root,
+// FP32 unsplit and tiled-march step kernels, built with --use_fast_math (approximate reciprocal and square root,
 // as the reference's own kernels are built, march_bridge/build_mhd.sh:25).  Two block shapes:
 // up to 256 threads with 2 resident blocks per SM (<= 128 registers), and up to 512 threads with
 // one block per SM for the larger tiles.
@@ -38,7 +38,19 @@ cudaError_t unsplit_prepare_f32() {
     for (int rc = 0; e == cudaSuccess && rc < 3; ++rc)
         e = launch_ensemble((const UnsplitArgs<float>*)nullptr, nullptr, 0, nullptr, rc == 2 ? RECON_PPM : RECON_MC,
                             rc == 0 ? RIEM_HLLD : RIEM_HLL, 1, 0);
+    UnsplitArgs<float> none{};
+    for (int rc = 0; e == cudaSuccess && rc < 2; ++rc) {
+        e = march_dispatch_t<float, 512, 1>(none, rc ? RECON_PPM : RECON_MC, 0, true);
+        if (e == cudaSuccess) e = march_dispatch_t<float, 256, 2>(none, rc ? RECON_PPM : RECON_MC, 0, true);
+    }
     return e;
+}
+cudaError_t launch_march_tiled(const UnsplitArgs<float>& A, int recon, cudaStream_t s) {
+    if (A.ox * A.oy > 256) return march_dispatch_t<float, 512, 1>(A, recon, s, false);
+    return march_dispatch_t<float, 256, 2>(A, recon, s, false);
+}
+int march_tiled_regs(const UnsplitArgs<float>*, int recon, int nthreads) {
+    return nthreads > 256 ? march_regs_of_t<float, 512, 1>(recon) : march_regs_of_t<float, 256, 2>(recon);
 }
 int unsplit_regs_f32(int recon, int riem, int nthreads) {
     return nthreads > 256 ? unsplit_regs_of_t<float, 512, 1>(recon, riem) : unsplit_regs_of_t<float, 256, 2>(recon, riem);

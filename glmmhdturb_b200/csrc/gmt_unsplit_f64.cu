@@ -12,9 +12,16 @@ cudaError_t unsplit_prepare_f64() {
     for (int rc = 0; e == cudaSuccess && rc < 3; ++rc)
         e = launch_ensemble((const UnsplitArgs<double>*)nullptr, nullptr, 0, nullptr, rc == 2 ? RECON_PPM : RECON_MC,
                             rc == 0 ? RIEM_HLLD : RIEM_HLL, 1, 0);
+    UnsplitArgs<double> none{};
+    for (int rc = 0; e == cudaSuccess && rc < 2; ++rc) e = march_dispatch_t<double, 256, 1>(none, rc ? RECON_PPM : RECON_MC, 0, true);
     return e;
 }
 int unsplit_regs_f64(int recon, int riem, int) { return unsplit_regs_of_t<double, 256, 1>(recon, riem); }
+cudaError_t launch_march_tiled(const UnsplitArgs<double>& A, int recon, cudaStream_t s) {
+    if (A.ox * A.oy > 256) return cudaErrorInvalidConfiguration;
+    return march_dispatch_t<double, 256, 1>(A, recon, s, false);
+}
+int march_tiled_regs(const UnsplitArgs<double>*, int recon, int) { return march_regs_of_t<double, 256, 1>(recon); }
 cudaError_t launch_ensemble(const UnsplitArgs<double>* boxes, const EnsItem* items, int nitems, unsigned* queue,
                             int recon, int riem, int nsm, cudaStream_t s) {
     if (recon == RECON_MC && riem == RIEM_HLLD) return ensemble_go<double, RECON_MC, RIEM_HLLD>(boxes, items, nitems, queue, nsm, s);

@@ -108,3 +108,34 @@ static cudaError_t ensemble_go(const UnsplitArgs<R>* boxes, const EnsItem* items
     return cudaGetLastError();
 }
 }  // namespace gmt
+
+namespace gmt {
+// tiled march launcher (recon MC or PPM; the march has no minmod variant, spike_mhd.cu:118-123);
+// nt <= 0 configures the kernel only
+template <class R, int RECON, int MAXT, int MINB>
+static cudaError_t march_go(const UnsplitArgs<R>& A, cudaStream_t s, bool configure_only) {
+    auto k = march_tile_kernel<R, RECON, MAXT, MINB>;
+    static int configured[64] = {0};
+    {
+        cudaError_t e = configure_once(k, configured);
+        if (e != cudaSuccess) return e;
+    }
+    if (configure_only) return cudaSuccess;
+    const int nt = A.ox * A.oy;
+    if (nt > MAXT || nt < 1) return cudaErrorInvalidConfiguration;
+    dim3 grid(A.nx / A.ox, A.ny / A.oy, (A.nz + A.lz - 1) / A.lz);
+    k<<<grid, nt, unsplit_smem_bytes<R>(A.ox, A.oy), s>>>(A);
+    return cudaGetLastError();
+}
+template <class R, int MAXT, int MINB>
+static cudaError_t march_dispatch_t(const UnsplitArgs<R>& A, int recon, cudaStream_t s, bool configure_only) {
+    if (recon == RECON_PPM) return march_go<R, RECON_PPM, MAXT, MINB>(A, s, configure_only);
+    return march_go<R, RECON_MC, MAXT, MINB>(A, s, configure_only);
+}
+template <class R, int MAXT, int MINB> static int march_regs_of_t(int recon) {
+    cudaFuncAttributes fa{};
+    cudaError_t e = recon == RECON_PPM ? cudaFuncGetAttributes(&fa, march_tile_kernel<R, RECON_PPM, MAXT, MINB>)
+                                       : cudaFuncGetAttributes(&fa, march_tile_kernel<R, RECON_MC, MAXT, MINB>);
+    return e == cudaSuccess ? fa.numRegs : -1;
+}
+}  // namespace gmt

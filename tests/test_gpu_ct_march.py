@@ -129,7 +129,7 @@ def test_ct_run_legacy_abi(golden):
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
 def test_march_passive_species_vs_oracle(oracle, recon, dtype):
     """Two passive species on the march scheme (CMA, spike_mhd.cu NSP): FP64 bit-exact against the
-    oracle, FP32 within 1e-5 of it; the MHD planes match the species-free step."""
+    oracle, FP32 within 1e-5 of it; the MHD planes match the species-free (tiled) step."""
     import math
     import numpy as np
     from glmmhdturb_b200 import Solver
@@ -154,7 +154,35 @@ def test_march_passive_species_vs_oracle(oracle, recon, dtype):
     else:
         err, errs = max_rel_err(got, ref)
         assert err <= 1e-5, errs
+    # without species the step runs the tiled march kernel: the same MHD planes (bit for bit in FP64;
+    # FP32 builds the tiled kernel with fast math)
     s9 = Solver(n, dtype=dtype, scheme="march1d", recon=recon, riemann="hll", gamma=5 / 3, smallp=cfg.smallp)
     o9 = torch.empty_like(ud[:9])
     s9.step(ud[:9].contiguous(), o9, dt, ch=smax, glm_fac=fac)
-    assert torch.equal(o9, out[:9])
+    if dtype == "f64":
+        assert torch.equal(o9, out[:9])
+    else:
+        err, errs = max_rel_err(o9.cpu().numpy(), ref[:9])
+        assert err <= 1e-5, errs
+
+
+@pytest.mark.parametrize("recon", ["mc", "ppm"])
+@pytest.mark.parametrize("n,tile", [((32, 24, 20), (0, 0, 0)), ((32, 32, 16), (16, 8, 5)), ((24, 16, 12), (8, 16, 0))])
+def test_tiled_march_vs_oracle(oracle, recon, n, tile):
+    """The tiled march kernel (one solve per face, z-march) against the oracle on non-cubic grids,
+    odd z-chunks and several tiles; FP64 bit-exact, and the fused CFL equals the oracle's."""
+    import math
+    from glmmhdturb_b200 import Solver
+    from tests.gpu_util import perturbed_glm_state
+    u0 = perturbed_glm_state(oracle, n, seed=9, gamma=5 / 3)
+    cfg = oracle.Config(n=n, gamma=5 / 3, recon=recon, riemann="hll")
+    cmax, smax = oracle.cfl(cfg, u0)
+    dt = 0.3 * cfg.dx / cmax
+    fac = math.exp(-(smax / 0.18) * dt)
+    ref = oracle.step_march1d(cfg, u0, dt, smax, fac)
+    s = Solver(n, dtype="f64", scheme="march1d", recon=recon, riemann="hll", gamma=5 / 3, smallp=cfg.smallp, tile=tile)
+    ud = to_dev(u0)
+    out = torch.empty_like(ud)
+    s.step(ud, out, dt, ch=smax, glm_fac=fac, want_cfl=True)
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)
+    assert s.cfl_result() == oracle.cfl(cfg, ref)
