@@ -109,8 +109,10 @@ template <class R> Consts<R> consts_of(const gmt_params& p) {
     return K;
 }
 
-int choose_tile(gmt_ctx* c) {
+int choose_tile(gmt_ctx* c, bool ct = false) {
     const gmt_params& p = c->p;
+    const int maxt = ct ? ct_max_threads(c->esize) : unsplit_max_threads(c->esize);
+    auto smem = [&](int ox, int oy) { return ct ? ct_smem_of(c->esize, ox, oy) : unsplit_smem(c->esize, ox, oy); };
     // largest first: 32x16 (512 threads, one block per SM) measured fastest at 512^3 FP32 for
     // both the unsplit and the march scheme; FP64 stops at 256 threads
     static const int cand[][2] = {{32, 16}, {32, 8}, {32, 4}, {16, 8}, {16, 4}, {8, 8}, {8, 4}, {4, 4},
@@ -119,8 +121,7 @@ int choose_tile(gmt_ctx* c) {
     if (ox <= 0 || oy <= 0) {
         ox = oy = 0;
         for (auto& t : cand)
-            if (divides(p.nx, t[0]) && divides(p.ny, t[1]) && t[0] * t[1] <= unsplit_max_threads(c->esize) &&
-                unsplit_smem(c->esize, t[0], t[1]) <= 227 * 1024) {
+            if (divides(p.nx, t[0]) && divides(p.ny, t[1]) && t[0] * t[1] <= maxt && smem(t[0], t[1]) <= 227 * 1024) {
                 ox = t[0];
                 oy = t[1];
                 break;
@@ -128,9 +129,8 @@ int choose_tile(gmt_ctx* c) {
     }
     if (!divides(p.nx, ox) || !divides(p.ny, oy))
         return fail(GMT_ERR_ARG, "tile " + std::to_string(ox) + "x" + std::to_string(oy) + " does not divide the grid");
-    if (ox * oy > unsplit_max_threads(c->esize))
-        return fail(GMT_ERR_ARG, "tile_x*tile_y must be <= " + std::to_string(unsplit_max_threads(c->esize)));
-    if (unsplit_smem(c->esize, ox, oy) > 227 * 1024) return fail(GMT_ERR_ARG, "tile needs more than 227 KB shared memory");
+    if (ox * oy > maxt) return fail(GMT_ERR_ARG, "tile_x*tile_y must be <= " + std::to_string(maxt));
+    if (smem(ox, oy) > 227 * 1024) return fail(GMT_ERR_ARG, "tile needs more than 227 KB shared memory");
     int lz = p.tile_z;
     if (lz <= 0) {
         long cols = (long)(p.nx / ox) * (p.ny / oy);
@@ -276,6 +276,7 @@ int ct_step_impl(gmt_ctx* c, const CPlanes8<R>& q, const Planes8<R>& o, const gm
     A.btab = a->do_turb ? static_cast<const R*>(c->btab) : nullptr;
     A.trigx = static_cast<const R*>(c->trig[0]);
     A.scratch = static_cast<R*>(c->ct_scratch);
+    A.err = c->err;
     cudaError_t e = launch_ct(A, s);
     if (e != cudaSuccess) return cuda_fail(e, "ct step");
     if (a->want_cfl) {
@@ -349,6 +350,7 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     if (g_mode_err != cudaSuccess) return cuda_fail(g_mode_err, "mode table");
     {
         cudaError_t e = p->dtype == GMT_F64 ? unsplit_prepare_f64() : unsplit_prepare_f32();
+        if (e == cudaSuccess && p->scheme == GMT_SCHEME_CT) e = p->dtype == GMT_F64 ? ct_prepare_f64() : ct_prepare_f32();
         if (e != cudaSuccess) return cuda_fail(e, "kernel attributes");
     }
 
@@ -359,6 +361,7 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     cudaGetDevice(&c->device);
     int rc = GMT_OK;
     if (p->scheme == GMT_SCHEME_UNSPLIT || (p->scheme == GMT_SCHEME_MARCH1D && p->nsp == 0)) rc = choose_tile(c);
+    if (p->scheme == GMT_SCHEME_CT) rc = choose_tile(c, true);
     if (rc != GMT_OK) { delete c; return rc; }
     auto alloc = [&](void** ptr, size_t bytes) -> bool {
         cudaError_t e = cudaMalloc(ptr, bytes);
@@ -372,7 +375,7 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
               alloc(&c->btab, (size_t)p->ny * p->nz * 24 * c->esize);
     const int dims[3] = {p->nx, p->ny, p->nz};
     for (int a = 0; ok && a < 3; ++a) ok = alloc(&c->trig[a], (size_t)8 * dims[a] * c->esize);
-    if (ok && p->scheme == GMT_SCHEME_CT) ok = alloc(&c->ct_scratch, (size_t)27 * c->n * c->esize);
+    if (ok && p->scheme == GMT_SCHEME_CT) ok = alloc(&c->ct_scratch, (size_t)15 * c->n * c->esize);
     if (ok) ok = alloc((void**)&c->divb, sizeof(unsigned long long));
     if (ok) ok = alloc((void**)&c->err, sizeof(int));
     if (ok) ok = alloc((void**)&c->loop, sizeof(LoopState)) && alloc((void**)&c->loopc, sizeof(LoopConst)) &&
@@ -459,7 +462,7 @@ int gmt_kernel_info(gmt_ctx* c, int32_t* regs, int64_t* smem, int32_t tile[3]) {
             sm = (int64_t)unsplit_smem(c->esize, c->ox, c->oy);
         }
     } else {
-        r = ct_regs_of(c->esize);
+        r = ct_regs_of(c->esize, c->p.recon, c->p.riemann, c->ox * c->oy);
         sm = (int64_t)ct_smem_of(c->esize, c->ox, c->oy);
     }
     if (regs) *regs = r;
@@ -1352,8 +1355,16 @@ double ct_run(float* const* qv, float* const* ov, float* const* cc, int nsteps) 
     return (double)ms;
 }
 
-int ct_regs(void) { return ct_regs_of(4); }
-int ct_shmem(void) { return (int)ct_smem_of(4, 0, 0); }
+int ct_regs(void) {
+    std::lock_guard<std::mutex> lk(g_legacy_mu);
+    gmt_ctx* c = legacy_ctx(1);
+    return c ? ct_regs_of(4, c->p.recon, c->p.riemann, c->ox * c->oy) : -1;
+}
+int ct_shmem(void) {
+    std::lock_guard<std::mutex> lk(g_legacy_mu);
+    gmt_ctx* c = legacy_ctx(1);
+    return c ? (int)ct_smem_of(4, c->ox, c->oy) : -1;
+}
 
 }  // extern "C"
 

@@ -1,0 +1,458 @@
+// gmt_ct_tile.cuh -- constrained-transport step as a z-marching tile kernel plus two short
+// per-cell passes (CTMHD.step!, ct_mhd.jl:174; the fused march of spike_ctm.cu:250-298).
+//
+// Pass A (ct_tile_kernel): a block owns an OX x OY column tile over LZ planes, exactly like the
+// GLM step.  Shared memory holds
+//   PR[3][9][(OX+4)(OY+4)]  cell primitives with the face-averaged field (ring of 3 planes),
+//   FB[3][3][(OX+4)(OY+4)]  the lower-face fields bxf, byf, bzf of the same cells,
+//   ST[4][9][(OX+2)(OY+2)]  in-plane interface states, overwritten by the face fluxes,
+//   SG[9][(OX+5)(OY+5)]     staging of plane k+2: 5 conserved, bxf, byf, bzf(k+2), bzf(k+3)
+// (one more row and column than the ring, for the face averages of the outermost cells).  Per
+// direction each cell gets a full (or ct_mhd.jl's half) MonCen slope, the transverse-free 1-D
+// Hancock predictor and its two face states, whose normal component is the face field; every
+// face is solved once (HLL or HLLD, no GLM).  The write-out does the hydro update with the
+// floor/kick epilogue (on the old cell-centred field) and stores, per cell, the EMF data of its
+// three lower faces and its cell-centre EMF: 12 planes of scratch.
+// Pass B1 (ct_edge_kernel): the edge EMFs -- Balsara-Spicer average (ct_mhd.jl:139-154) or the
+// upwind contact EMF of Gardiner & Stone (2005) -- from that scratch, in the oracle's order.
+// Pass B2 (ct_face_kernel): face B advances by the curl of the edge EMFs (ct_mhd.jl:156-172), so
+// the face divergence is preserved to round-off.
+#pragma once
+#include "gmt_internal.h"
+#include "gmt_unsplit_inst.cuh"
+#include <algorithm>
+
+namespace gmt {
+
+// scratch plane indices (each n reals)
+enum CTScratch {
+    CS_EZX = 0,   // -F_x[By]  on the lower x face   (E_z on an x face)
+    CS_EYX,       // +F_x[Bz]                        (E_y on an x face)
+    CS_MX,        //  F_x[rho]
+    CS_EXY,       // -F_y[Bz]  on the lower y face   (E_x on a y face)
+    CS_EZY,       // +F_y[Bx]                        (E_z on a y face)
+    CS_MY,        //  F_y[rho]
+    CS_EYZ,       // -F_z[Bx]  on the lower z face   (E_y on a z face)
+    CS_EXZ,       // +F_z[By]                        (E_x on a z face)
+    CS_MZ,        //  F_z[rho]
+    CS_ECX,       // cell-centre E = -(v x B)
+    CS_ECY,
+    CS_ECZ,
+    CS_EDX,       // edge EMFs ex (i, j-1/2, k-1/2), ey (i-1/2, j, k-1/2), ez (i-1/2, j-1/2, k)
+    CS_EDY,
+    CS_EDZ,
+    CS_PLANES
+};
+
+// byte offset of the reduction / mbarrier words: after the real arrays, rounded up to 16 bytes
+template <class R> __host__ __device__ inline size_t ct_tile_words_offset(int ox, int oy) {
+    size_t PN = (size_t)(ox + 4) * (oy + 4), RN = (size_t)(ox + 2) * (oy + 2), PN5 = (size_t)(ox + 5) * (oy + 5);
+    return ((27 * PN + 9 * PN + 36 * RN + 9 * PN5) * sizeof(R) + 15) / 16 * 16;
+}
+template <class R> __host__ __device__ inline size_t ct_tile_smem_bytes(int ox, int oy) {
+    return ct_tile_words_offset<R>(ox, oy) + 40 * sizeof(double);
+}
+
+// stage plane kp: the conserved cell variables, the three face fields at kp and bzf at kp+1, on
+// the region x0-2..x0+OX+2, y0-2..y0+OY+2
+template <class R>
+__device__ __forceinline__ void ct_stage_plane(R* __restrict__ SG, const CPlanes8<R>& q, int PN5, int PW5, int x0,
+                                               int y0, int kp, int nx, int ny, int nz, int tid, int nt) {
+    const size_t gz = (size_t)wrapi(kp, nz), gz1 = (size_t)wrapi(kp + 1, nz);
+    for (int c = tid; c < PN5; c += nt) {
+        const int lx = c % PW5, ly = c / PW5;
+        const size_t gxy = (size_t)wrapi(x0 - 2 + lx, nx) + (size_t)nx * wrapi(y0 - 2 + ly, ny);
+        const size_t g = gxy + (size_t)nx * ny * gz, g1 = gxy + (size_t)nx * ny * gz1;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) cp_async_r(SG + v * PN5 + c, q.p[v] + g);
+        cp_async_r(SG + 8 * PN5 + c, q.p[7] + g1);
+    }
+    cp_async_commit();
+}
+
+// staged plane -> primitives with the face-averaged field (ct_mhd.jl:85-97) and the lower faces
+template <class R>
+__device__ __forceinline__ void ct_unstage_plane(R* __restrict__ PRs, R* __restrict__ FBs, const R* __restrict__ SG,
+                                                 int PN, int PW, int PN5, int PW5, const Consts<R>& K, int tid, int nt) {
+    for (int c = tid; c < PN; c += nt) {
+        const int lx = c % PW, ly = c / PW;
+        const int c5 = lx + PW5 * ly;
+        Q9<R> cu;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) cu.v[v] = SG[v * PN5 + c5];
+        const R bxl = SG[5 * PN5 + c5], byl = SG[6 * PN5 + c5], bzl = SG[7 * PN5 + c5];
+        cu.v[5] = R(0.5) * (bxl + SG[5 * PN5 + c5 + 1]);
+        cu.v[6] = R(0.5) * (byl + SG[6 * PN5 + c5 + PW5]);
+        cu.v[7] = R(0.5) * (bzl + SG[8 * PN5 + c5]);
+        cu.v[8] = R(0);
+        const Q9<R> q = cons2prim(cu, K.gamma, K.smallr, K.smallp);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) PRs[v * PN + c] = q.v[v];
+        FBs[0 * PN + c] = bxl;
+        FBs[1 * PN + c] = byl;
+        FBs[2 * PN + c] = bzl;
+    }
+}
+
+// one cell's slope and 1-D predictor along D (spike_ctm / ct_mhd.jl:40-80)
+template <class R> struct CTCell {
+    Q9<R> m0, s, mh;
+};
+
+template <int D, class R>
+__device__ __forceinline__ void ct_neighbours(const R* PR, int PN, int PW, int c, int s0, int sm, int sp, Q9<R>& L,
+                                              Q9<R>& Rr) {
+    const R* PL = PR + (size_t)(D == 2 ? sm : s0) * 9 * PN;
+    const R* PP = PR + (size_t)(D == 2 ? sp : s0) * 9 * PN;
+    const int cl = D == 0 ? c - 1 : (D == 1 ? c - PW : c), cr = D == 0 ? c + 1 : (D == 1 ? c + PW : c);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) { L.v[v] = PL[v * PN + cl]; Rr.v[v] = PP[v * PN + cr]; }
+}
+
+template <int D, class R>
+__device__ __forceinline__ void ct_prep(CTCell<R>& r, const R* PR, int PN, int PW, int c, int s0, int sm, int sp,
+                                        const Consts<R>& K, R dtdx, int halfslope) {
+    Q9<R> L, Rr;
+    ct_neighbours<D>(PR, PN, PW, c, s0, sm, sp, L, Rr);
+    r.s = full_slope(L, r.m0, Rr);
+    if (halfslope) {
+#pragma unroll
+        for (int v = 0; v < 9; ++v) r.s.v[v] = R(0.5) * r.s.v[v];
+    }
+    r.mh = hanc1d<D>(r.m0, r.s, dtdx, K.gamma, K.smallr, K.smallp);
+}
+
+// face state on the SIGN side along D, floored, with the face normal field bn
+template <int D, int SIGN, int RECON, class R>
+__device__ __forceinline__ Q9<R> ct_state(const CTCell<R>& r, const R* PR, int PN, int PW, int c, int s0, int sm,
+                                          int sp, const Consts<R>& K, R bn) {
+    Q9<R> f;
+    if (RECON == RECON_PPM) {
+        Q9<R> L, Rr;
+        ct_neighbours<D>(PR, PN, PW, c, s0, sm, sp, L, Rr);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            R lo, hi;
+            ppm_edges(L.v[v], r.m0.v[v], Rr.v[v], lo, hi);
+            f.v[v] = (SIGN > 0 ? hi : lo) + r.mh.v[v] - r.m0.v[v];
+        }
+    } else {
+        f = padd(r.mh, r.s, SIGN > 0 ? R(0.5) : R(-0.5));
+    }
+    f.v[0] = rmax(f.v[0], K.smallr);
+    f.v[4] = rmax(f.v[4], K.smallp);
+    f.v[5 + D] = bn;
+    f.v[8] = R(0);
+    return f;
+}
+
+template <int D, int RIEM, class R>
+__device__ __forceinline__ Q9<R> ct_flux(const Q9<R>& L, const Q9<R>& Rr, const Consts<R>& K) {
+    const Q9<R> Lr = rot_to<D>(L), Rrr = rot_to<D>(Rr);
+    const R bn = Lr.v[5];
+    return rot_from<D>(RIEM == RIEM_HLLD ? hlld_x(Lr, Rrr, K.gamma, bn, R(0), R(0))
+                                         : hll_x(Lr, Rrr, K.gamma, bn, R(0), R(0)));
+}
+
+template <class R, int RECON, int RIEM, int TOX, int TOY>
+__device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int bz, unsigned char* smem_raw) {
+    const int OX = TOX > 0 ? TOX : A.ox, OY = TOY > 0 ? TOY : A.oy;
+    const int PW = OX + 4, PN = (OX + 4) * (OY + 4);
+    const int PW5 = OX + 5, PN5 = (OX + 5) * (OY + 5);
+    const int RW = OX + 2, RN = (OX + 2) * (OY + 2);
+    R* PR = reinterpret_cast<R*>(smem_raw);
+    R* FB = PR + 27 * PN;
+    R* ST = FB + 9 * PN;
+    R* SG = ST + 36 * RN;
+    double* red = reinterpret_cast<double*>(smem_raw + ct_tile_words_offset<R>(OX, OY));
+
+    const int tid = threadIdx.x, NT = OX * OY;
+    const int tx = tid % OX, ty = tid / OX;
+    const int x0 = bx * OX, y0 = by * OY;
+    const int z0 = bz * A.lz, z1 = min(z0 + A.lz, A.nz);
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const size_t n = (size_t)nx * ny * nz;
+    const Consts<R> K = A.K;
+    const R dtdx = A.dtdx;
+    const bool turb = A.do_turb && A.btab != nullptr;
+    const int nhelp = 2 * (OX + OY);
+    R* S = A.scratch;
+
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
+    for (int j = 0; j < 3; ++j) {
+        ct_stage_plane(SG, A.q, PN5, PW5, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
+        cp_async_wait_all();
+        __syncthreads();
+        ct_unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, FB + mod3(z0 - 2 + j) * 3 * PN, SG, PN, PW, PN5, PW5, K, tid,
+                         NT);
+        if (j == 2 && tid == 0) mbar_init(mbar, NT);
+        __syncthreads();
+    }
+
+    Q9<R> pPz, Fzlo, Fxh, Fyh;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) { pPz.v[v] = R(0); Fzlo.v[v] = R(0); Fxh.v[v] = R(0); Fyh.v[v] = R(0); }
+    const int gx = x0 + tx, gy = y0 + ty;
+    const int cown = (tx + 2) + PW * (ty + 2);
+    const int rown = (tx + 1) + RW * (ty + 1);
+    const int ixh = (tx + 2) + RW * (ty + 1);
+    const int iyh = (tx + 1) + RW * (ty + 2);
+    unsigned phase = 0;
+
+    for (int kr = z0 - 1; kr <= z1; ++kr) {
+        const bool first = kr == z0 - 1, last = kr == z1;
+        const bool load = kr + 2 <= z1 + 1;
+        const int s0 = mod3(kr), sm = mod3(kr - 1), sp = mod3(kr + 1);
+        const R* FB0 = FB + (size_t)s0 * 3 * PN;
+        if (load) {
+            ct_stage_plane(SG, A.q, PN5, PW5, x0, y0, kr + 2, nx, ny, nz, tid, NT);
+            mbar_arrive_cp_async(mbar);
+        }
+        {
+            Q9<R> XY, Fxl, Fyl;
+            if (kr - 1 >= z0) {
+                Fxl = st_get(ST + 1 * 9 * RN, RN, rown);
+                Fyl = st_get(ST + 3 * 9 * RN, RN, rown);
+#pragma unroll
+                for (int v = 0; v < 9; ++v) XY.v[v] = (Fxl.v[v] - Fxh.v[v]) + (Fyl.v[v] - Fyh.v[v]);
+            }
+            CTCell<R> r;
+            {
+                const R* P0 = PR + (size_t)s0 * 9 * PN;
+#pragma unroll
+                for (int v = 0; v < 9; ++v) r.m0.v[v] = P0[v * PN + cown];
+            }
+            if (!first && !last) {
+                ct_prep<0>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx, A.halfslope);
+                st_put(ST + 0 * 9 * RN, RN, rown,
+                       ct_state<0, +1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[0 * PN + cown + 1]));
+                st_put(ST + 1 * 9 * RN, RN, rown,
+                       ct_state<0, -1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[0 * PN + cown]));
+                ct_prep<1>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx, A.halfslope);
+                st_put(ST + 2 * 9 * RN, RN, rown,
+                       ct_state<1, +1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[1 * PN + cown + PW]));
+                st_put(ST + 3 * 9 * RN, RN, rown,
+                       ct_state<1, -1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[1 * PN + cown]));
+            }
+            ct_prep<2>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx, A.halfslope);
+            const R* FBp = FB + (size_t)sp * 3 * PN;
+            Q9<R> Pz = ct_state<2, +1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FBp[2 * PN + cown]);
+            if (!first) {
+                Q9<R> Mz = ct_state<2, -1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[2 * PN + cown]);
+                Q9<R> Fzhi = ct_flux<2, RIEM>(pPz, Mz, K);
+                if (kr - 1 >= z0) {
+                    const int kf = kr - 1;
+                    const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * kf);
+                    const R* Pm = PR + (size_t)sm * 9 * PN;
+                    Q9<R> q;
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) q.v[v] = A.q.p[v][g] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
+                    // the epilogue sees the old cell-centred field
+                    const R vx = Pm[1 * PN + cown], vy = Pm[2 * PN + cown], vz = Pm[3 * PN + cown];
+                    const R bxc = Pm[5 * PN + cown], byc = Pm[6 * PN + cown], bzc = Pm[7 * PN + cown];
+                    q.v[5] = bxc; q.v[6] = byc; q.v[7] = bzc; q.v[8] = R(0);
+                    R ax = R(0), ay = R(0), az = R(0);
+                    if (turb) force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, A.ramp, ax, ay, az);
+                    finish_update(q, K, R(1), turb, ax, ay, az, A.dt);
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) A.o.p[v][g] = q.v[v];
+                    // EMF data of the three lower faces and the cell-centre EMF (-(v x B))
+                    S[CS_EZX * n + g] = -Fxl.v[6];
+                    S[CS_EYX * n + g] = Fxl.v[7];
+                    S[CS_MX * n + g] = Fxl.v[0];
+                    S[CS_EXY * n + g] = -Fyl.v[7];
+                    S[CS_EZY * n + g] = Fyl.v[5];
+                    S[CS_MY * n + g] = Fyl.v[0];
+                    S[CS_EYZ * n + g] = -Fzlo.v[5];
+                    S[CS_EXZ * n + g] = Fzlo.v[6];
+                    S[CS_MZ * n + g] = Fzlo.v[0];
+                    S[CS_ECX * n + g] = -(vy * bzc - vz * byc);
+                    S[CS_ECY * n + g] = -(vz * bxc - vx * bzc);
+                    S[CS_ECZ * n + g] = -(vx * byc - vy * bxc);
+                }
+                Fzlo = Fzhi;
+            }
+            pPz = Pz;
+        }
+        if (!first && !last) {
+            // halo cells: the one interface state each contributes to the tile's faces
+            for (int h = tid; h < nhelp; h += NT) {
+                int rc, cc, which;
+                if (h < OY) { rc = 0 + RW * (h + 1); cc = 1 + PW * (h + 2); which = 0; }
+                else if (h < 2 * OY) { int f = h - OY; rc = (OX + 1) + RW * (f + 1); cc = (OX + 2) + PW * (f + 2); which = 1; }
+                else if (h < 2 * OY + OX) { int f = h - 2 * OY; rc = (f + 1); cc = (f + 2) + PW * 1; which = 2; }
+                else { int f = h - 2 * OY - OX; rc = (f + 1) + RW * (OY + 1); cc = (f + 2) + PW * (OY + 2); which = 3; }
+                CTCell<R> r;
+                {
+                    const R* P0 = PR + (size_t)s0 * 9 * PN;
+#pragma unroll
+                    for (int v = 0; v < 9; ++v) r.m0.v[v] = P0[v * PN + cc];
+                }
+                Q9<R> f;
+                if (which < 2) {
+                    ct_prep<0>(r, PR, PN, PW, cc, s0, sm, sp, K, dtdx, A.halfslope);
+                    if (which == 0) f = ct_state<0, +1, RECON>(r, PR, PN, PW, cc, s0, sm, sp, K, FB0[0 * PN + cc + 1]);
+                    else f = ct_state<0, -1, RECON>(r, PR, PN, PW, cc, s0, sm, sp, K, FB0[0 * PN + cc]);
+                } else {
+                    ct_prep<1>(r, PR, PN, PW, cc, s0, sm, sp, K, dtdx, A.halfslope);
+                    if (which == 2) f = ct_state<1, +1, RECON>(r, PR, PN, PW, cc, s0, sm, sp, K, FB0[1 * PN + cc + PW]);
+                    else f = ct_state<1, -1, RECON>(r, PR, PN, PW, cc, s0, sm, sp, K, FB0[1 * PN + cc]);
+                }
+                st_put(ST + which * 9 * RN, RN, rc, f);
+            }
+        }
+        __syncthreads();
+        if (!first && !last) {
+            Fxh = ct_flux<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, rown), st_get(ST + 1 * 9 * RN, RN, ixh), K);
+            st_put(ST + 1 * 9 * RN, RN, ixh, Fxh);
+            Fyh = ct_flux<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, rown), st_get(ST + 3 * 9 * RN, RN, iyh), K);
+            st_put(ST + 3 * 9 * RN, RN, iyh, Fyh);
+            for (int h = NT - 1 - tid; h < OX + OY; h += NT) {
+                if (h < OY) {
+                    const int il = 0 + RW * (h + 1), ir = 1 + RW * (h + 1);
+                    st_put(ST + 1 * 9 * RN, RN, ir, ct_flux<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, il), st_get(ST + 1 * 9 * RN, RN, ir), K));
+                } else {
+                    const int c = h - OY;
+                    const int il = (c + 1), ir = (c + 1) + RW;
+                    st_put(ST + 3 * 9 * RN, RN, ir, ct_flux<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, il), st_get(ST + 3 * 9 * RN, RN, ir), K));
+                }
+            }
+        }
+        if (load) {
+            mbar_wait(mbar, phase, A.err);
+            phase ^= 1u;
+            ct_unstage_plane(PR + mod3(kr + 2) * 9 * PN, FB + mod3(kr + 2) * 3 * PN, SG, PN, PW, PN5, PW5, K, tid, NT);
+        }
+        __syncthreads();
+    }
+    if (tid == 0) mbar_inval(mbar);
+}
+
+template <class R, int RECON, int RIEM, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) ct_tile_kernel(const CTArgs<R> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ct_tile<R, RECON, RIEM, 0, 0>(A, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
+template <class R> __device__ __forceinline__ R ct_upwind(R flux, R minus, R plus) {
+    return flux > R(0) ? minus : (flux < R(0) ? plus : R(0.5) * (minus + plus));
+}
+
+// Pass B1: the three edge EMFs of cell (i,j,k) -- ez at (i-1/2, j-1/2, k), ex at (i, j-1/2, k-1/2),
+// ey at (i-1/2, j, k-1/2) -- for the cyclic axes (A, B, e): on the A-face the face EMF is
+// -F_A[B_B], on the B-face +F_B[B_A]; the same expressions and order as the oracle.
+template <class R> __global__ void __launch_bounds__(256) ct_edge_kernel(const CTArgs<R> A) {
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const size_t n = (size_t)nx * ny * nz;
+    const R* S = A.scratch;
+    R* W = A.scratch;
+    const bool contact = A.emf == 1;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((size_t)nx * ny));
+        const size_t xm = (size_t)wrapi(x - 1, nx) + (size_t)nx * (y + (size_t)ny * z);
+        const size_t ym = (size_t)x + (size_t)nx * (wrapi(y - 1, ny) + (size_t)ny * z);
+        const size_t zm = (size_t)x + (size_t)nx * (y + (size_t)ny * wrapi(z - 1, nz));
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            // A = (e+1)%3, B = (e+2)%3; c10 = one step back along A, c01 along B, c11 along both
+            size_t c10, c01, c11;
+            int ea, eb, ma, mb, ec;
+            if (e == 2) {        // (A,B) = (x,y)
+                c10 = xm; c01 = ym;
+                c11 = (size_t)wrapi(x - 1, nx) + (size_t)nx * (wrapi(y - 1, ny) + (size_t)ny * z);
+                ea = CS_EZX; eb = CS_EZY; ma = CS_MX; mb = CS_MY; ec = CS_ECZ;
+            } else if (e == 0) { // (A,B) = (y,z)
+                c10 = ym; c01 = zm;
+                c11 = (size_t)x + (size_t)nx * (wrapi(y - 1, ny) + (size_t)ny * wrapi(z - 1, nz));
+                ea = CS_EXY; eb = CS_EXZ; ma = CS_MY; mb = CS_MZ; ec = CS_ECX;
+            } else {             // (A,B) = (z,x)
+                c10 = zm; c01 = xm;
+                c11 = (size_t)wrapi(x - 1, nx) + (size_t)nx * (y + (size_t)ny * wrapi(z - 1, nz));
+                ea = CS_EYZ; eb = CS_EYX; ma = CS_MZ; mb = CS_MX; ec = CS_ECY;
+            }
+            const R EaN = S[ea * n + c], EaS = S[ea * n + c01];
+            const R EbE = S[eb * n + c], EbW = S[eb * n + c10];
+            R E = R(0.25) * (EbE + EbW + EaN + EaS);
+            if (contact) {
+                const R e00 = S[ec * n + c], e10 = S[ec * n + c10], e01 = S[ec * n + c01], e11 = S[ec * n + c11];
+                const R dN = ct_upwind(S[ma * n + c], e10 - EbW, e00 - EbE);
+                const R dS = ct_upwind(S[ma * n + c01], EbW - e11, EbE - e01);
+                const R dE = ct_upwind(S[mb * n + c], e01 - EaS, e00 - EaN);
+                const R dW = ct_upwind(S[mb * n + c10], EaS - e11, EaN - e10);
+                E = E + R(0.25) * (dS - dN) + R(0.25) * (dW - dE);
+            }
+            W[(CS_EDX + e) * n + c] = E;
+        }
+    }
+}
+
+// Pass B2: face B by the curl of the edge EMFs
+template <class R> __global__ void __launch_bounds__(256) ct_face_kernel(const CTArgs<R> A) {
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const size_t n = (size_t)nx * ny * nz;
+    const R* ex = A.scratch + CS_EDX * n;
+    const R* ey = A.scratch + CS_EDY * n;
+    const R* ez = A.scratch + CS_EDZ * n;
+    const R dtdx = A.dtdx;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((size_t)nx * ny));
+        const size_t cxp = (size_t)wrapi(x + 1, nx) + (size_t)nx * (y + (size_t)ny * z);
+        const size_t cyp = (size_t)x + (size_t)nx * (wrapi(y + 1, ny) + (size_t)ny * z);
+        const size_t czp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrapi(z + 1, nz));
+        A.o.p[5][c] = A.q.p[5][c] - dtdx * ((ez[cyp] - ez[c]) - (ey[czp] - ey[c]));
+        A.o.p[6][c] = A.q.p[6][c] - dtdx * ((ex[czp] - ex[c]) - (ez[cxp] - ez[c]));
+        A.o.p[7][c] = A.q.p[7][c] - dtdx * ((ey[cxp] - ey[c]) - (ex[cyp] - ex[c]));
+    }
+}
+
+// launch: pass A (tile kernel), then B1 and B2; nt <= 0 in A configures the kernel only
+template <class R, int RECON, int RIEM, int MAXT, int MINB>
+static cudaError_t ct_go(const CTArgs<R>& A, cudaStream_t s, bool configure_only) {
+    auto k = ct_tile_kernel<R, RECON, RIEM, MAXT, MINB>;
+    static int configured[64] = {0};
+    {
+        cudaError_t e = configure_once(k, configured);
+        if (e != cudaSuccess) return e;
+    }
+    if (configure_only) return cudaSuccess;
+    const int nt = A.ox * A.oy;
+    if (nt > MAXT || nt < 1) return cudaErrorInvalidConfiguration;
+    dim3 grid(A.nx / A.ox, A.ny / A.oy, (A.nz + A.lz - 1) / A.lz);
+    k<<<grid, nt, ct_tile_smem_bytes<R>(A.ox, A.oy), s>>>(A);
+    const size_t n = (size_t)A.nx * A.ny * A.nz;
+    const int nb = (int)std::min<size_t>((n + 255) / 256, (size_t)148 * 16);
+    ct_edge_kernel<R><<<nb, 256, 0, s>>>(A);
+    ct_face_kernel<R><<<nb, 256, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+template <class R, int MAXT, int MINB>
+static cudaError_t ct_dispatch_t(const CTArgs<R>& A, int recon, int riem, cudaStream_t s, bool configure_only) {
+    const bool ppm = recon == RECON_PPM, hlld = riem == RIEM_HLLD;
+    if (ppm && hlld) return ct_go<R, RECON_PPM, RIEM_HLLD, MAXT, MINB>(A, s, configure_only);
+    if (ppm) return ct_go<R, RECON_PPM, RIEM_HLL, MAXT, MINB>(A, s, configure_only);
+    if (hlld) return ct_go<R, RECON_MC, RIEM_HLLD, MAXT, MINB>(A, s, configure_only);
+    return ct_go<R, RECON_MC, RIEM_HLL, MAXT, MINB>(A, s, configure_only);
+}
+
+template <class R, int MAXT, int MINB> static cudaError_t ct_configure_all_t() {
+    CTArgs<R> none{};
+    cudaError_t e = cudaSuccess;
+    for (int rc = 0; e == cudaSuccess && rc < 2; ++rc)
+        for (int rm = 0; e == cudaSuccess && rm < 2; ++rm)
+            e = ct_dispatch_t<R, MAXT, MINB>(none, rc ? RECON_PPM : RECON_MC, rm ? RIEM_HLL : RIEM_HLLD, 0, true);
+    return e;
+}
+
+template <class R, int MAXT, int MINB> static int ct_regs_of_t(int recon, int riem) {
+    cudaFuncAttributes fa{};
+    const bool ppm = recon == RECON_PPM, hlld = riem == RIEM_HLLD;
+    cudaError_t e;
+    if (ppm && hlld) e = cudaFuncGetAttributes(&fa, ct_tile_kernel<R, RECON_PPM, RIEM_HLLD, MAXT, MINB>);
+    else if (ppm) e = cudaFuncGetAttributes(&fa, ct_tile_kernel<R, RECON_PPM, RIEM_HLL, MAXT, MINB>);
+    else if (hlld) e = cudaFuncGetAttributes(&fa, ct_tile_kernel<R, RECON_MC, RIEM_HLLD, MAXT, MINB>);
+    else e = cudaFuncGetAttributes(&fa, ct_tile_kernel<R, RECON_MC, RIEM_HLL, MAXT, MINB>);
+    return e == cudaSuccess ? fa.numRegs : -1;
+}
+
+}  // namespace gmt

@@ -57,12 +57,16 @@ template <class R> struct CTArgs {
     int recon, riem, emf, halfslope, do_turb;
     const R* btab;
     const R* trigx;
-    R* scratch;            // 27 planes: lower-face fluxes F[3][8] and edge EMFs E[3]
+    R* scratch;            // 15 planes: lower-face EMF data and cell EMFs (12), edge EMFs (3)
+    int* err;              // device flag set when a bounded wait gives up
 };
 cudaError_t launch_ct(const CTArgs<float>& A, cudaStream_t s);
 cudaError_t launch_ct(const CTArgs<double>& A, cudaStream_t s);
-int ct_regs_of(int dtype_bytes);
+cudaError_t ct_prepare_f32();   // shared-memory attributes of the CT tile kernels
+cudaError_t ct_prepare_f64();
+int ct_regs_of(int dtype_bytes, int recon, int riem, int nthreads);
 size_t ct_smem_of(int dtype_bytes, int ox, int oy);
+int ct_max_threads(int dtype_bytes);
 
 // auxiliary kernels (gmt_aux.cu)
 template <class R> cudaError_t launch_cfl(const CPlanes<R>& u, size_t n, const Consts<R>& K,
