@@ -24,6 +24,7 @@
 #pragma once
 #include "gmt_dual.cuh"
 #include "gmt_internal.h"
+#include "gmt_riemann_adj.cuh"
 
 namespace gmt {
 
@@ -182,9 +183,15 @@ template <int RIEM, class R>
 GMT_HD void riemann_adj(const Q9<R>& L, const Q9<R>& Rr, const Q9<R>& Fb, int d, const Consts<R>& K, R ch,
                         bool use_llf, Q9<R>& Lb, Q9<R>& Rb) {
     using DD = Dual<R, NCH>;
-    const Consts<DD> KD = dual_consts<R, NCH>(K);
     const Q9<R> Lx = rot_to_d(L, d), Rx = rot_to_d(Rr, d), Fbx = rot_to_d(Fb, d);
     Q9<R> Lbx = q9_zero<R>(), Rbx = q9_zero<R>();
+    // hand-written reverse sweep (HLLD, HLL); the exact-speed LLF paths go through dual numbers
+    if (riemann_x_adj<RIEM>(Lx, Rx, Fbx, K, ch, use_llf, Lbx, Rbx)) {
+        Lb = rot_from_d(Lbx, d);
+        Rb = rot_from_d(Rbx, d);
+        return;
+    }
+    const Consts<DD> KD = dual_consts<R, NCH>(K);
 #pragma unroll 1
     for (int c0 = 0; c0 < 18; c0 += NCH) {
         Q9<DD> Ld, Rd;

@@ -907,6 +907,10 @@ int gmt_run(gmt_ctx* c, void* u, void* w, int32_t nsteps, double t0, double t_en
 // ------------------------------------------------------------------------------------------
 }  // extern "C"
 
+// z-chunk of an ensemble work item: 32 planes keep the per-chunk prologue (two extra planes) near
+// 6% while a 64-box ensemble still yields thousands of items for the persistent grid
+constexpr int ENS_LZ = 32;
+
 struct gmt_ensemble {
     gmt_params p;
     int nbox = 0;
@@ -947,7 +951,7 @@ template <class R> int ens_bind(gmt_ensemble* E, void* const* u, void* const* w,
             a.u = cplanes<R>(par == 0 ? u[b] : w[b], cells);
             a.o = planes<R>(par == 0 ? w[b] : u[b], cells);
             a.nx = a.ny = a.nz = n;
-            a.ox = 16; a.oy = 16; a.lz = 16;
+            a.ox = 16; a.oy = 16; a.lz = ENS_LZ;
             a.dt = a.dtdx = a.ch = a.glm_fac = a.ramp = R(0);
             a.K = consts_of<R>(E->p);
             a.iflo = E->p.iflo; a.use_llf = E->p.riemann == GMT_RIEMANN_LLF;
@@ -1054,13 +1058,14 @@ int gmt_ensemble_create(const gmt_params* base, int32_t nbox, const int32_t* n, 
         for (int a = 0; a < 3; ++a) A(&E->trig[3 * b + a], (size_t)8 * n[b] * E->esize);
         E->rows_max = std::max(E->rows_max, n[b] * n[b]);
     }
-    // work items: biggest boxes first, 16x16 tiles x 16-plane chunks
+    // work items: biggest boxes first, 16x16 tiles x ENS_LZ-plane chunks (the last chunk of a box
+    // may be shorter)
     std::vector<int> order(nbox);
     for (int b = 0; b < nbox; ++b) order[b] = b;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
     std::vector<EnsItem> items;
     for (int b : order)
-        for (int bz = 0; bz < n[b] / 16; ++bz)
+        for (int bz = 0; bz < (n[b] + ENS_LZ - 1) / ENS_LZ; ++bz)
             for (int by = 0; by < n[b] / 16; ++by)
                 for (int bx = 0; bx < n[b] / 16; ++bx) items.push_back({b, bx, by, bz});
     E->nitems = (int)items.size();
