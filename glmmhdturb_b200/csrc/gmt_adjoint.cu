@@ -1,66 +1,8 @@
-// gmt_adjoint.cu -- the six grid-stride kernels of the discrete adjoint of the unsplit step (one
-// thread per cell; the per-cell passes are in gmt_adjoint.cuh) and their launcher.
-#include <algorithm>
-
-#include "gmt_adjoint.cuh"
+// gmt_adjoint.cu -- FP64 instantiation of the adjoint kernels (gmt_adjoint_kern.cuh), built with
+// --fmad=false like the FP64 forward step.
+#include "gmt_adjoint_kern.cuh"
 
 namespace gmt {
-
-#define GMT_ADJ_LOOP for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
-
-template <class R> __global__ void __launch_bounds__(128) adj_faces_kernel(const AdjArgs<R> A) {
-    const size_t n = (size_t)A.nx * A.ny * A.nz;
-    GMT_ADJ_LOOP adj_faces_cell(A, c);
-}
-template <int RIEM, class R> __global__ void __launch_bounds__(128) adj_flux_kernel(const AdjArgs<R> A) {
-    const size_t n = (size_t)A.nx * A.ny * A.nz;
-    GMT_ADJ_LOOP adj_flux_cell<RIEM>(A, c);
-}
-template <class R> __global__ void __launch_bounds__(128) adj_update_kernel(const AdjArgs<R> A) {
-    const size_t n = (size_t)A.nx * A.ny * A.nz;
-    __shared__ double red[128];
-    double damp = 0.0;
-    GMT_ADJ_LOOP damp += adj_update_cell(A, c);
-    red[threadIdx.x] = damp;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0 && A.damp) atomicAdd(A.damp, red[0]);
-}
-template <int RIEM, class R> __global__ void __launch_bounds__(128) adj_riemann_kernel(const AdjArgs<R> A) {
-    const size_t n = (size_t)A.nx * A.ny * A.nz;
-    GMT_ADJ_LOOP adj_riemann_cell<RIEM>(A, c);
-}
-template <class R> __global__ void __launch_bounds__(128) adj_recon_kernel(const AdjArgs<R> A) {
-    const size_t n = (size_t)A.nx * A.ny * A.nz;
-    GMT_ADJ_LOOP adj_recon_cell(A, c);
-}
-template <class R> __global__ void __launch_bounds__(128) adj_gather_kernel(const AdjArgs<R> A) {
-    const size_t n = (size_t)A.nx * A.ny * A.nz;
-    GMT_ADJ_LOOP adj_gather_cell(A, c);
-}
-
 size_t adjoint_scratch_reals(size_t n) { return (size_t)(54 + 27 + 9 + 54 + 63) * n; }
-
-template <class R> cudaError_t launch_adjoint(const AdjArgs<R>& A, cudaStream_t s) {
-    const size_t n = (size_t)A.nx * A.ny * A.nz;
-    const int nb = (int)std::min<size_t>((n + 127) / 128, 148 * 16);
-    adj_faces_kernel<R><<<nb, 128, 0, s>>>(A);
-    if (A.riem == RIEM_HLL) adj_flux_kernel<RIEM_HLL, R><<<nb, 128, 0, s>>>(A);
-    else if (A.riem == RIEM_LLF_BOUND) adj_flux_kernel<RIEM_LLF_BOUND, R><<<nb, 128, 0, s>>>(A);
-    else adj_flux_kernel<RIEM_HLLD, R><<<nb, 128, 0, s>>>(A);
-    adj_update_kernel<R><<<nb, 128, 0, s>>>(A);
-    if (A.riem == RIEM_HLL) adj_riemann_kernel<RIEM_HLL, R><<<nb, 128, 0, s>>>(A);
-    else if (A.riem == RIEM_LLF_BOUND) adj_riemann_kernel<RIEM_LLF_BOUND, R><<<nb, 128, 0, s>>>(A);
-    else adj_riemann_kernel<RIEM_HLLD, R><<<nb, 128, 0, s>>>(A);
-    adj_recon_kernel<R><<<nb, 128, 0, s>>>(A);
-    adj_gather_kernel<R><<<nb, 128, 0, s>>>(A);
-    return cudaGetLastError();
-}
-
-template cudaError_t launch_adjoint<float>(const AdjArgs<float>&, cudaStream_t);
 template cudaError_t launch_adjoint<double>(const AdjArgs<double>&, cudaStream_t);
-
 }  // namespace gmt

@@ -12,13 +12,13 @@
 //              [F_d(m0+s_d) - F_d(m0-s_d)]) by one vector-Jacobian product per flux; limiter
 //              derivatives split each slope bar onto the three cells of its stencil
 //   6 gather   qbar(c) = own + neighbours' slope terms; ubar += (dq/du)^T qbar
-// The Riemann solvers, the directional fluxes, the epilogue, prim2cons and cons2prim are
+// The Riemann solves (HLLD, HLL), the directional fluxes, prim2cons and cons2prim have hand-written
+// reverse sweeps (gmt_riemann_adj.cuh); the exact-speed LLF paths and the update epilogue are
 // differentiated by running the forward physics functions on forward-mode duals seeded in chunks
-// (the seeds are selects on a chunk offset, so no tangent is ever indexed dynamically); each
-// vector-Jacobian product is exact for the code that ran forward.  The limiter derivative, the
-// face/revert structure, the Hancock sum and the flux-difference identity are written out.  At a
-// limiter kink, an HLLD fan switch, a floor or an interface-state revert the derivative of the
-// branch that was taken is used (a subgradient).
+// (the seeds are selects on a chunk offset, so no tangent is ever indexed dynamically).  The
+// limiter derivative, the face/revert structure, the Hancock sum and the flux-difference identity
+// are written out.  At a limiter kink, an HLLD fan switch, a floor or an interface-state revert the
+// derivative of the branch that was taken is used (a subgradient).
 //
 // Every pass is a host-device function of one cell, so the same code also runs on the host.
 #pragma once
@@ -30,35 +30,6 @@ namespace gmt {
 
 
 constexpr int NCH = 3;   // tangents per dual pass
-
-// xbar = (df/dx)^T ybar for f: 9 -> 9, by forward-mode passes of NC tangents each
-template <int NC, class R, class Fn> GMT_HD Q9<R> vjp9(Fn f, const Q9<R>& x, const Q9<R>& yb) {
-    using DD = Dual<R, NC>;
-    Q9<R> xb;
-#pragma unroll
-    for (int v = 0; v < 9; ++v) xb.v[v] = R(0);
-#pragma unroll 1
-    for (int c0 = 0; c0 < 9; c0 += NC) {
-        Q9<DD> xd;
-#pragma unroll
-        for (int v = 0; v < 9; ++v) {
-            xd.v[v] = DD(x.v[v]);
-#pragma unroll
-            for (int j = 0; j < NC; ++j) xd.v[v].d[j] = (c0 + j == v) ? R(1) : R(0);
-        }
-        Q9<DD> y = f(xd);
-#pragma unroll
-        for (int j = 0; j < NC; ++j) {
-            R acc = R(0);
-#pragma unroll
-            for (int v = 0; v < 9; ++v) acc += yb.v[v] * y.v[v].d[j];
-#pragma unroll
-            for (int v = 0; v < 9; ++v)
-                if (c0 + j == v) xb.v[v] = acc;
-        }
-    }
-    return xb;
-}
 
 template <class R> GMT_HD void q9_add(Q9<R>& a, const Q9<R>& b, R s = R(1)) {
 #pragma unroll
@@ -179,14 +150,17 @@ GMT_HD Q9<R> riemann_dir(const Q9<R>& L, const Q9<R>& Rr, int d, const Consts<R>
 
 // Lbar, Rbar = J^T Fbar of the Riemann solve at a face of direction d (18 inputs in chunks of NCH,
 // evaluated in the x frame)
-template <int RIEM, class R>
+// DUALS: whether the exact-speed LLF paths can occur (LLF-bound solver, use_llf, or the density /
+// pressure LLF switch); without them every face takes the hand-written reverse sweep and the
+// dual-number code is not compiled in
+template <int RIEM, bool DUALS, class R>
 GMT_HD void riemann_adj(const Q9<R>& L, const Q9<R>& Rr, const Q9<R>& Fb, int d, const Consts<R>& K, R ch,
                         bool use_llf, Q9<R>& Lb, Q9<R>& Rb) {
     using DD = Dual<R, NCH>;
     const Q9<R> Lx = rot_to_d(L, d), Rx = rot_to_d(Rr, d), Fbx = rot_to_d(Fb, d);
     Q9<R> Lbx = q9_zero<R>(), Rbx = q9_zero<R>();
     // hand-written reverse sweep (HLLD, HLL); the exact-speed LLF paths go through dual numbers
-    if (riemann_x_adj<RIEM>(Lx, Rx, Fbx, K, ch, use_llf, Lbx, Rbx)) {
+    if (riemann_x_adj<RIEM>(Lx, Rx, Fbx, K, ch, use_llf, Lbx, Rbx) || !DUALS) {
         Lb = rot_from_d(Lbx, d);
         Rb = rot_from_d(Rbx, d);
         return;
@@ -236,21 +210,6 @@ template <class R> GMT_HD Q9<R> fs_get(const R* FS, size_t n, size_t c, int k) {
     for (int v = 0; v < 9; ++v) q.v[v] = FS[(size_t)(k * 9 + v) * n + c];
     return q;
 }
-
-template <class R> struct FluxXFn {   // the x-normal ideal MHD flux
-    R gamma;
-    template <class T> GMT_HD Q9<T> operator()(const Q9<T>& q) const { return phys_flux_x(q, T(gamma)); }
-};
-template <class R> struct C2PFn {
-    Consts<R> K;
-    template <class T> GMT_HD Q9<T> operator()(const Q9<T>& q) const {
-        return cons2prim(q, T(K.gamma), T(K.smallr), T(K.pfl));
-    }
-};
-template <class R> struct P2CFn {
-    R gamma;
-    template <class T> GMT_HD Q9<T> operator()(const Q9<T>& q) const { return prim2cons(q, T(gamma)); }
-};
 
 // pass 1: the six interface states of cell c
 template <class R> GMT_HD void adj_faces_cell(const AdjArgs<R>& A, size_t c) {
@@ -344,7 +303,7 @@ template <class R> GMT_HD double adj_update_cell(const AdjArgs<R>& A, size_t c) 
 }
 
 // pass 4: adjoint of the Riemann solves at the +x, +y, +z faces of cell c
-template <int RIEM, class R> GMT_HD void adj_riemann_cell(const AdjArgs<R>& A, size_t c) {
+template <int RIEM, bool DUALS, class R> GMT_HD void adj_riemann_cell(const AdjArgs<R>& A, size_t c) {
     const Idx<R> I = idx_of(A);
     const bool ul = A.use_llf != 0;
     int x, y, z;
@@ -356,7 +315,7 @@ template <int RIEM, class R> GMT_HD void adj_riemann_cell(const AdjArgs<R>& A, s
 #pragma unroll
         for (int v = 0; v < 9; ++v) Fb.v[v] = A.dtdx * (A.R1b[(size_t)v * I.n + cp] - A.R1b[(size_t)v * I.n + c]);
         const Q9<R> L = fs_get(A.FS, I.n, c, 2 * d), Rr = fs_get(A.FS, I.n, cp, 2 * d + 1);
-        riemann_adj<RIEM>(L, Rr, Fb, d, A.K, A.ch, ul, Lb, Rb);
+        riemann_adj<RIEM, DUALS>(L, Rr, Fb, d, A.K, A.ch, ul, Lb, Rb);
 #pragma unroll
         for (int v = 0; v < 9; ++v) {
             A.FSb[(size_t)((2 * d) * 9 + v) * I.n + c] = Lb.v[v];
@@ -393,18 +352,21 @@ template <class R> GMT_HD void adj_recon_cell(const AdjArgs<R>& A, size_t c) {
     if (r.hrev) {
         q9_add(m0b, mhb);
     } else {
-        const Q9<R> uhb = vjp9<3>(C2PFn<R>{A.K}, r.uh, mhb);
-        q9_add(m0b, vjp9<3>(P2CFn<R>{A.K.gamma}, r.m0, uhb));
+        Q9<R> uhb = q9_zero<R>();
+        cons2prim_adj(r.uh, A.K.gamma, A.K.smallr, A.K.pfl, mhb, uhb);
+        prim2cons_adj(r.m0, A.K.gamma, uhb, m0b);
         Q9<R> Fb;
         const R h = R(0.5) * A.dtdx;
 #pragma unroll
         for (int v = 0; v < 9; ++v) Fb.v[v] = -h * uhb.v[v];
-#pragma unroll 1
+#pragma unroll
         for (int d = 0; d < 3; ++d) {
             // dir_flux<d> = rot_from_d . phys_flux_x . rot_to_d
             const Q9<R> Fbx = rot_to_d(Fb, d);
-            const Q9<R> jp = rot_from_d(vjp9<3>(FluxXFn<R>{A.K.gamma}, rot_to_d(padd(r.m0, r.s[d], R(1)), d), Fbx), d);
-            const Q9<R> jm = rot_from_d(vjp9<3>(FluxXFn<R>{A.K.gamma}, rot_to_d(padd(r.m0, r.s[d], R(-1)), d), Fbx), d);
+            Q9<R> jpx = q9_zero<R>(), jmx = q9_zero<R>();
+            phys_flux_x_adj(rot_to_d(padd(r.m0, r.s[d], R(1)), d), A.K.gamma, Fbx, jpx);
+            phys_flux_x_adj(rot_to_d(padd(r.m0, r.s[d], R(-1)), d), A.K.gamma, Fbx, jmx);
+            const Q9<R> jp = rot_from_d(jpx, d), jm = rot_from_d(jmx, d);
 #pragma unroll
             for (int v = 0; v < 9; ++v) {
                 m0b.v[v] += jp.v[v] - jm.v[v];
@@ -445,7 +407,8 @@ template <class R> GMT_HD void adj_gather_cell(const AdjArgs<R>& A, size_t c) {
             s += -A.QB[(size_t)(9 + 9 * d + v) * I.n + cp[d]] + A.QB[(size_t)(36 + 9 * d + v) * I.n + cm[d]];
         qb.v[v] = s;
     }
-    const Q9<R> ubq = vjp9<3>(C2PFn<R>{A.K}, load_u(A.u, c), qb);
+    Q9<R> ubq = q9_zero<R>();
+    cons2prim_adj(load_u(A.u, c), A.K.gamma, A.K.smallr, A.K.pfl, qb, ubq);
 #pragma unroll
     for (int v = 0; v < 9; ++v) A.ub.p[v][c] += ubq.v[v];
 }

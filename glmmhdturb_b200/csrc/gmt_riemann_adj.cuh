@@ -1,6 +1,7 @@
-// gmt_riemann_adj.cuh -- hand-written reverse sweeps of the GLM Riemann solve in the x-normal frame:
-// the ideal-MHD flux, the fast speed, HLL and the Miyoshi-Kusano HLLD (gmt_phys.cuh; glmmhd_turb.jl:
-// 89-115, 193-272, 335-354), the GLM pair and the state floors of riemann_glm.
+// gmt_riemann_adj.cuh -- hand-written reverse sweeps of the step's physics functions: cons2prim and
+// prim2cons, the ideal-MHD flux, the fast speed, HLL and the Miyoshi-Kusano HLLD (gmt_phys.cuh;
+// glmmhd_turb.jl:68-115, 193-272, 335-354), and of riemann_glm (GLM pair and state floors) in the
+// x-normal frame.
 //
 // Each function re-evaluates the forward expressions it needs and then propagates the adjoint of
 // its outputs back to its inputs.  The branch conventions are those of the dual numbers and of
@@ -76,6 +77,31 @@ template <class R> GMT_HD void phys_flux_x_adj(const Q9<R>& q, R gamma, const Q9
     bx_b += b2_b * R(2) * bx; by_b += b2_b * R(2) * by; bz_b += b2_b * R(2) * bz;
     qb.v[0] += rho_b; qb.v[1] += vx_b; qb.v[2] += vy_b; qb.v[3] += vz_b; qb.v[4] += p_b;
     qb.v[5] += bx_b; qb.v[6] += by_b; qb.v[7] += bz_b;
+}
+
+// cb += adjoint of cons2prim(c, gamma, smallr, pf) for output adjoint qb
+template <class R>
+GMT_HD void cons2prim_adj(const Q9<R>& c, R gamma, R smallr, R pf, const Q9<R>& qb, Q9<R>& cb) {
+    const R rho = rmax(c.v[0], smallr);
+    const R ir = R(1) / rho;
+    const R msq = c.v[1] * c.v[1] + c.v[2] * c.v[2] + c.v[3] * c.v[3];
+    const R ekin = R(0.5) * msq * ir;
+    const R emag = R(0.5) * (c.v[5] * c.v[5] + c.v[6] * c.v[6] + c.v[7] * c.v[7]);
+    const R pr = (gamma - R(1)) * (c.v[4] - ekin - emag);
+    const R pr_b = qb.v[4] * sel_ge(pr, pf);
+    const R g1 = pr_b * (gamma - R(1));
+    const R ekin_b = -g1, emag_b = -g1;
+    cb.v[4] += g1;
+    cb.v[5] += qb.v[5] + emag_b * c.v[5];
+    cb.v[6] += qb.v[6] + emag_b * c.v[6];
+    cb.v[7] += qb.v[7] + emag_b * c.v[7];
+    cb.v[8] += qb.v[8];
+    cb.v[1] += qb.v[1] * ir + ekin_b * c.v[1] * ir;
+    cb.v[2] += qb.v[2] * ir + ekin_b * c.v[2] * ir;
+    cb.v[3] += qb.v[3] * ir + ekin_b * c.v[3] * ir;
+    const R ir_b = qb.v[1] * c.v[1] + qb.v[2] * c.v[2] + qb.v[3] * c.v[3] + ekin_b * R(0.5) * msq;
+    const R rho_b = qb.v[0] - ir_b * ir * ir;
+    cb.v[0] += rho_b * sel_ge(c.v[0], smallr);
 }
 
 // qb += adjoint of prim2cons(q, gamma) for output adjoint ub (the psi slot passes through)
@@ -228,6 +254,113 @@ template <class R> GMT_HD void hside_u_adj(const HSide<R>& s, const R* ub, HSide
     b.E += ub[4]; bn_b += ub[5]; b.by += ub[6]; b.bz += ub[7];
 }
 
+// outer region of the HLLD fan on side s: F = F_s + S_s (U*_s - U_s)
+template <class R>
+GMT_HD void hlld_outer_adj(HSide<R>& s, HSideB<R>& b, R ds, R SM, R pts, R bn, const R* g, Q9<R>& Fb, R& ds_b,
+                           R& SM_b, R& pts_b, R& bn_b) {
+    hside_star(s, SM, pts, bn);
+    const R Us[9] = {ds, ds * SM, ds * s.vys, ds * s.vzs, s.Es, bn, s.bys, s.bzs, R(0)};
+    const R U[9] = {s.d, s.d * s.u, s.d * s.v, s.d * s.w, s.E, bn, s.by, s.bz, R(0)};
+    R Usb[9], Ub[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        b.S += g[i] * (Us[i] - U[i]);
+        Usb[i] = g[i] * s.S;
+        Ub[i] = -g[i] * s.S;
+        Fb.v[i] = g[i];
+    }
+    ds_b += Usb[0] + Usb[1] * SM + Usb[2] * s.vys + Usb[3] * s.vzs;
+    SM_b += Usb[1] * ds;
+    b.vys += Usb[2] * ds;
+    b.vzs += Usb[3] * ds;
+    b.Es += Usb[4];
+    bn_b += Usb[5];
+    b.bys += Usb[6];
+    b.bzs += Usb[7];
+    hside_u_adj(s, Ub, b, bn_b);
+    hside_star_adj(s, SM, pts, bn, b, SM_b, pts_b, bn_b);
+}
+
+// inner region: F = F_s + S*s Uss - (S*s - S_s) Us - S_s U on the sampled side s (LO: the left
+// side, SM >= 0; else the right side); both star states are already evaluated
+template <bool LO, class R>
+GMT_HD void hlld_inner_adj(const HSide<R>& sl, const HSide<R>& sr, HSideB<R>& bl, HSideB<R>& br, R ds, R sqdLs,
+                           R sqdRs, R Ssx, R SM, R pts, R bn, const R* g, Q9<R>& Fb, R& ds_b, R& sqdLs_b, R& sqdRs_b,
+                           R& Ssx_b, R& SM_b, R& bn_b) {
+    const HSide<R>& s = LO ? sl : sr;
+    HSideB<R>& b = LO ? bl : br;
+    const R sgn = bn >= R(0) ? R(1) : R(-1);
+    const R ssum = sqdLs + sqdRs;
+    const R invsum = R(1) / ssum;
+    const R nvy = sqdLs * sl.vys + sqdRs * sr.vys + (sr.bys - sl.bys) * sgn;
+    const R nvz = sqdLs * sl.vzs + sqdRs * sr.vzs + (sr.bzs - sl.bzs) * sgn;
+    const R nby = sqdLs * sr.bys + sqdRs * sl.bys + sqdLs * sqdRs * (sr.vys - sl.vys) * sgn;
+    const R nbz = sqdLs * sr.bzs + sqdRs * sl.bzs + sqdLs * sqdRs * (sr.vzs - sl.vzs) * sgn;
+    const R vyss = nvy * invsum, vzss = nvz * invsum, byss = nby * invsum, bzss = nbz * invsum;
+    const R vdotbss = SM * bn + vyss * byss + vzss * bzss;
+    const R sq = LO ? sqdLs : sqdRs;
+    const R sign_e = LO ? R(-1) : R(1);   // ELss = ELs - sq(.)sgn, ERss = ERs + sq(.)sgn
+    const R Ess = s.Es + sign_e * (sq * (s.vdotbs - vdotbss) * sgn);
+    const R Uss[9] = {ds, ds * SM, ds * vyss, ds * vzss, Ess, bn, byss, bzss, R(0)};
+    const R Us[9] = {ds, ds * SM, ds * s.vys, ds * s.vzs, s.Es, bn, s.bys, s.bzs, R(0)};
+    const R U[9] = {s.d, s.d * s.u, s.d * s.v, s.d * s.w, s.E, bn, s.by, s.bz, R(0)};
+    R Ussb[9], Usb[9], Ub[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        Ssx_b += g[i] * (Uss[i] - Us[i]);
+        b.S += g[i] * (Us[i] - U[i]);
+        Ussb[i] = g[i] * Ssx;
+        Usb[i] = -g[i] * (Ssx - s.S);
+        Ub[i] = -g[i] * s.S;
+        Fb.v[i] = g[i];
+    }
+    // Uss
+    ds_b += Ussb[0] + Ussb[1] * SM + Ussb[2] * vyss + Ussb[3] * vzss;
+    SM_b += Ussb[1] * ds;
+    R vyss_b = Ussb[2] * ds, vzss_b = Ussb[3] * ds;
+    const R Ess_b = Ussb[4];
+    bn_b += Ussb[5];
+    R byss_b = Ussb[6], bzss_b = Ussb[7];
+    // Ess = Es + sign_e * sq * (vdotbs - vdotbss) * sgn
+    b.Es += Ess_b;
+    (LO ? sqdLs_b : sqdRs_b) += Ess_b * sign_e * (s.vdotbs - vdotbss) * sgn;
+    b.vdotbs += Ess_b * sign_e * sq * sgn;
+    const R vdotbss_b = -Ess_b * sign_e * sq * sgn;
+    // vdotbss = SM bn + vyss byss + vzss bzss
+    SM_b += vdotbss_b * bn;
+    bn_b += vdotbss_b * SM;
+    vyss_b += vdotbss_b * byss; byss_b += vdotbss_b * vyss;
+    vzss_b += vdotbss_b * bzss; bzss_b += vdotbss_b * vzss;
+    // Us (the sampled side's star state) and U
+    ds_b += Usb[0] + Usb[1] * SM + Usb[2] * s.vys + Usb[3] * s.vzs;
+    SM_b += Usb[1] * ds;
+    b.vys += Usb[2] * ds;
+    b.vzs += Usb[3] * ds;
+    b.Es += Usb[4];
+    bn_b += Usb[5];
+    b.bys += Usb[6];
+    b.bzs += Usb[7];
+    hside_u_adj(s, Ub, b, bn_b);
+    // the double-star averages
+    const R invsum_b = vyss_b * nvy + vzss_b * nvz + byss_b * nby + bzss_b * nbz;
+    const R tvy = vyss_b * invsum, tvz = vzss_b * invsum, tby = byss_b * invsum, tbz = bzss_b * invsum;
+    sqdLs_b += tvy * sl.vys + tvz * sl.vzs + tby * sr.bys + tbz * sr.bzs + tby * sqdRs * (sr.vys - sl.vys) * sgn +
+               tbz * sqdRs * (sr.vzs - sl.vzs) * sgn;
+    sqdRs_b += tvy * sr.vys + tvz * sr.vzs + tby * sl.bys + tbz * sl.bzs + tby * sqdLs * (sr.vys - sl.vys) * sgn +
+               tbz * sqdLs * (sr.vzs - sl.vzs) * sgn;
+    bl.vys += tvy * sqdLs - tby * sqdLs * sqdRs * sgn;
+    br.vys += tvy * sqdRs + tby * sqdLs * sqdRs * sgn;
+    bl.vzs += tvz * sqdLs - tbz * sqdLs * sqdRs * sgn;
+    br.vzs += tvz * sqdRs + tbz * sqdLs * sqdRs * sgn;
+    bl.bys += -tvy * sgn + tby * sqdRs;
+    br.bys += tvy * sgn + tby * sqdLs;
+    bl.bzs += -tvz * sgn + tbz * sqdRs;
+    br.bzs += tvz * sgn + tbz * sqdLs;
+    const R ssum_b = -invsum_b * invsum * invsum;
+    sqdLs_b += ssum_b;
+    sqdRs_b += ssum_b;
+}
+
 // HLLD (hlld_x): Lb, Rb, bnb += adjoint for flux adjoint fb (fb[5], fb[8] do not enter)
 template <class R>
 GMT_HD void hlld_x_adj(const Q9<R>& L, const Q9<R>& Rr, R gamma, R bn, const Q9<R>& fb, Q9<R>& Lb, Q9<R>& Rb, R& bnb) {
@@ -269,121 +402,19 @@ GMT_HD void hlld_x_adj(const Q9<R>& L, const Q9<R>& Rr, R gamma, R bn, const Q9<
     Q9<R> FLb, FRb;
 #pragma unroll
     for (int i = 0; i < 9; ++i) { FLb.v[i] = R(0); FRb.v[i] = R(0); }
-    const bool left = SLs >= R(0), right = !left && SRs < R(0);
-    if (left || right) {
-        // F = F_s + S_s (U*_s - U_s) on the outer side s
-        HSide<R>& s = left ? sl : sr;
-        HSideB<R>& b = left ? bl : br;
-        const R ds = left ? dLs : dRs;
-        hside_star(s, SM, pts, bn);
-        const R Us[9] = {ds, ds * SM, ds * s.vys, ds * s.vzs, s.Es, bn, s.bys, s.bzs, R(0)};
-        const R U[9] = {s.d, s.d * s.u, s.d * s.v, s.d * s.w, s.E, bn, s.by, s.bz, R(0)};
-        R Usb[9], Ub[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            b.S += g[i] * (Us[i] - U[i]);
-            Usb[i] = g[i] * s.S;
-            Ub[i] = -g[i] * s.S;
-        }
-        Q9<R>& Fb = left ? FLb : FRb;
-#pragma unroll
-        for (int i = 0; i < 9; ++i) Fb.v[i] = g[i];
-        R& dsb = left ? dLs_b : dRs_b;
-        dsb += Usb[0] + Usb[1] * SM + Usb[2] * s.vys + Usb[3] * s.vzs;
-        SM_b += Usb[1] * ds;
-        b.vys += Usb[2] * ds;
-        b.vzs += Usb[3] * ds;
-        b.Es += Usb[4];
-        bn_b += Usb[5];
-        b.bys += Usb[6];
-        b.bzs += Usb[7];
-        hside_u_adj(s, Ub, b, bn_b);
-        hside_star_adj(s, SM, pts, bn, b, SM_b, pts_b, bn_b);
+    if (SLs >= R(0)) {
+        hlld_outer_adj(sl, bl, dLs, SM, pts, bn, g, FLb, dLs_b, SM_b, pts_b, bn_b);
+    } else if (SRs < R(0)) {
+        hlld_outer_adj(sr, br, dRs, SM, pts, bn, g, FRb, dRs_b, SM_b, pts_b, bn_b);
     } else {
-        // inner fan: both star states and the double-star state
         hside_star(sl, SM, pts, bn);
         hside_star(sr, SM, pts, bn);
-        const R sgn = bn >= R(0) ? R(1) : R(-1);
-        const R ssum = sqdLs + sqdRs;
-        const R invsum = R(1) / ssum;
-        const R nvy = sqdLs * sl.vys + sqdRs * sr.vys + (sr.bys - sl.bys) * sgn;
-        const R nvz = sqdLs * sl.vzs + sqdRs * sr.vzs + (sr.bzs - sl.bzs) * sgn;
-        const R nby = sqdLs * sr.bys + sqdRs * sl.bys + sqdLs * sqdRs * (sr.vys - sl.vys) * sgn;
-        const R nbz = sqdLs * sr.bzs + sqdRs * sl.bzs + sqdLs * sqdRs * (sr.vzs - sl.vzs) * sgn;
-        const R vyss = nvy * invsum, vzss = nvz * invsum, byss = nby * invsum, bzss = nbz * invsum;
-        const R vdotbss = SM * bn + vyss * byss + vzss * bzss;
-        const bool lo = SM >= R(0);
-        HSide<R>& s = lo ? sl : sr;
-        HSideB<R>& b = lo ? bl : br;
-        const R ds = lo ? dLs : dRs;
-        const R sq = lo ? sqdLs : sqdRs;
-        const R Ssx = lo ? SLs : SRs;                 // inner wave speed of the sampled side
-        const R sign_e = lo ? R(-1) : R(1);           // ELss = ELs - sq(.)sgn, ERss = ERs + sq(.)sgn
-        const R Ess = s.Es + sign_e * (sq * (s.vdotbs - vdotbss) * sgn);
-        const R Uss[9] = {ds, ds * SM, ds * vyss, ds * vzss, Ess, bn, byss, bzss, R(0)};
-        const R Us[9] = {ds, ds * SM, ds * s.vys, ds * s.vzs, s.Es, bn, s.bys, s.bzs, R(0)};
-        const R U[9] = {s.d, s.d * s.u, s.d * s.v, s.d * s.w, s.E, bn, s.by, s.bz, R(0)};
-        // F = F_s + S*s Uss - (S*s - S_s) Us - S_s U
-        R Ussb[9], Usb[9], Ub[9], Ssx_b = R(0);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            Ssx_b += g[i] * (Uss[i] - Us[i]);
-            b.S += g[i] * (Us[i] - U[i]);
-            Ussb[i] = g[i] * Ssx;
-            Usb[i] = -g[i] * (Ssx - s.S);
-            Ub[i] = -g[i] * s.S;
-        }
-        if (lo) SLs_b += Ssx_b; else SRs_b += Ssx_b;
-        Q9<R>& Fb = lo ? FLb : FRb;
-#pragma unroll
-        for (int i = 0; i < 9; ++i) Fb.v[i] = g[i];
-        R& dsb = lo ? dLs_b : dRs_b;
-        // Uss
-        dsb += Ussb[0] + Ussb[1] * SM + Ussb[2] * vyss + Ussb[3] * vzss;
-        SM_b += Ussb[1] * ds;
-        R vyss_b = Ussb[2] * ds, vzss_b = Ussb[3] * ds;
-        const R Ess_b = Ussb[4];
-        bn_b += Ussb[5];
-        R byss_b = Ussb[6], bzss_b = Ussb[7];
-        // Ess = Es + sign_e * sq * (vdotbs - vdotbss) * sgn
-        b.Es += Ess_b;
-        R& sqb = lo ? sqdLs_b : sqdRs_b;
-        sqb += Ess_b * sign_e * (s.vdotbs - vdotbss) * sgn;
-        b.vdotbs += Ess_b * sign_e * sq * sgn;
-        const R vdotbss_b = -Ess_b * sign_e * sq * sgn;
-        // vdotbss = SM bn + vyss byss + vzss bzss
-        SM_b += vdotbss_b * bn;
-        bn_b += vdotbss_b * SM;
-        vyss_b += vdotbss_b * byss; byss_b += vdotbss_b * vyss;
-        vzss_b += vdotbss_b * bzss; bzss_b += vdotbss_b * vzss;
-        // Us (the sampled side's star state)
-        dsb += Usb[0] + Usb[1] * SM + Usb[2] * s.vys + Usb[3] * s.vzs;
-        SM_b += Usb[1] * ds;
-        b.vys += Usb[2] * ds;
-        b.vzs += Usb[3] * ds;
-        b.Es += Usb[4];
-        bn_b += Usb[5];
-        b.bys += Usb[6];
-        b.bzs += Usb[7];
-        hside_u_adj(s, Ub, b, bn_b);
-        // the double-star averages
-        const R invsum_b = vyss_b * nvy + vzss_b * nvz + byss_b * nby + bzss_b * nbz;
-        const R tvy = vyss_b * invsum, tvz = vzss_b * invsum, tby = byss_b * invsum, tbz = bzss_b * invsum;
-        sqdLs_b += tvy * sl.vys + tvz * sl.vzs + tby * sr.bys + tbz * sr.bzs +
-                   tby * sqdRs * (sr.vys - sl.vys) * sgn + tbz * sqdRs * (sr.vzs - sl.vzs) * sgn;
-        sqdRs_b += tvy * sr.vys + tvz * sr.vzs + tby * sl.bys + tbz * sl.bzs +
-                   tby * sqdLs * (sr.vys - sl.vys) * sgn + tbz * sqdLs * (sr.vzs - sl.vzs) * sgn;
-        bl.vys += tvy * sqdLs - tby * sqdLs * sqdRs * sgn;
-        br.vys += tvy * sqdRs + tby * sqdLs * sqdRs * sgn;
-        bl.vzs += tvz * sqdLs - tbz * sqdLs * sqdRs * sgn;
-        br.vzs += tvz * sqdRs + tbz * sqdLs * sqdRs * sgn;
-        bl.bys += -tvy * sgn + tby * sqdRs;
-        br.bys += tvy * sgn + tby * sqdLs;
-        bl.bzs += -tvz * sgn + tbz * sqdRs;
-        br.bzs += tvz * sgn + tbz * sqdLs;
-        const R ssum_b = -invsum_b * invsum * invsum;
-        sqdLs_b += ssum_b;
-        sqdRs_b += ssum_b;
+        if (SM >= R(0))
+            hlld_inner_adj<true>(sl, sr, bl, br, dLs, sqdLs, sqdRs, SLs, SM, pts, bn, g, FLb, dLs_b, sqdLs_b, sqdRs_b,
+                                 SLs_b, SM_b, bn_b);
+        else
+            hlld_inner_adj<false>(sl, sr, bl, br, dRs, sqdLs, sqdRs, SRs, SM, pts, bn, g, FRb, dRs_b, sqdLs_b, sqdRs_b,
+                                  SRs_b, SM_b, bn_b);
         hside_star_adj(sl, SM, pts, bn, bl, SM_b, pts_b, bn_b);
         hside_star_adj(sr, SM, pts, bn, br, SM_b, pts_b, bn_b);
     }
