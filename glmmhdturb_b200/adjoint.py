@@ -180,9 +180,14 @@ class StepFunction(torch.autograd.Function):
         return gin, None, None, None, None, None, None
 
 
+def adjoint_scratch_bytes(solver: Solver) -> int:
+    """Device bytes the context's adjoint scratch holds (207 state planes)."""
+    return 207 * solver.n * (8 if solver.dtype_name == "f64" else 4)
+
+
 def dot(a: torch.Tensor, b: torch.Tensor) -> float:
     return float((a.double() * b.double()).sum())
 
 
 __all__ = ["Schedule", "StepRecord", "StepFunction", "forward", "replay", "backward", "ke_band_gradient",
-           "checkpoint_interval", "velocity_b_direction", "dot"]
+           "checkpoint_interval", "velocity_b_direction", "adjoint_scratch_bytes", "dot"]

@@ -280,3 +280,25 @@ def test_configs3_forward_mode_directions_fp64(oracle):
         assert _rel(fwd, adj) <= 1e-8, (k, fwd, adj)
     fwd_amp = float((gN * du[7]).sum()) / 2.0
     assert _rel(fwd_amp, r["grad_amp"]) <= 1e-8, (fwd_amp, r["grad_amp"])
+
+
+def test_configs4_adjoint_128cube_200_steps_in_40gb():
+    """The large adjoint: 128^3 FP32, 200 forced steps, checkpoint interval from a 40 GB budget
+    with recomputation; finite gradients, device memory within the budget."""
+    import time
+    from glmmhdturb_b200 import adjoint as AD
+    n, nsteps, budget = 128, 200, 40 << 30
+    s, u0, d = _forced_base(n, seed=2, dtype="f32")
+    state_bytes = u0.numel() * u0.element_size()
+    K = AD.checkpoint_interval(nsteps, state_bytes, budget)
+    free0, total = torch.cuda.mem_get_info()
+    torch.cuda.reset_peak_memory_stats()
+    t0 = time.perf_counter()
+    r = AD.ke_band_gradient(s, u0, nsteps, kmin=4, kmax=8, checkpoint_every=K)
+    torch.cuda.synchronize()
+    elapsed = time.perf_counter() - t0
+    peak = torch.cuda.max_memory_allocated() + AD.adjoint_scratch_bytes(s)
+    print(f"configs[4] adjoint 128^3 x {nsteps}: K={K}, {elapsed:.2f} s forward+backward, "
+          f"peak {peak / 2**30:.2f} GB (torch tensors + adjoint scratch), dL/damp {r['grad_amp']:.4e}")
+    assert math.isfinite(r["grad_amp"]) and bool(torch.isfinite(r["grad_u0"]).all())
+    assert peak <= budget
