@@ -8,9 +8,12 @@ with the forcing kick.  Initial state: seeded synthetic turbulence (rms Mach 1, 
 p 0.6, B0 = (0.775, 0, 0)) standing in for the pre-evolved checkpoint of the 512^3 configuration.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--scheme unsplit|ct|march1d] [--n N] [--dtype f32|f64] [--recon mc|ppm] [--riemann hlld|hll]
 
 N > 1 runs under torchrun as independent replicas (the step has no cross-box exchange).
-Prints one JSON line on rank 0.
+Prints one JSON line on rank 0.  --scheme ct times the constrained-transport step (tile march,
+edge EMFs, face-B curl, CFL) from a divergence-free turbulent state; --scheme march1d the march
+scheme behind march_run_dev (no forcing).
 """
 from __future__ import annotations
 
@@ -32,6 +35,9 @@ COURANT = 0.3
 CP_COEF = 0.18
 GAMMA = 5.0 / 3.0
 BYTES_PER_ZONE = {"f32": 72, "f64": 144}   # read 9 + write 9 conserved reals per zone update
+# kernels of one step with the next step's CFL: the fused GLM / march step; CT's tile march, edge-EMF
+# pass, face-B pass and CFL reduction
+STEP_LAUNCHES = {"unsplit": 1, "march1d": 1, "ct": 4}
 PUBLISHED_A6000 = 0.902e9   # full step with fused OU forcing @512^3 FP32, RTX A6000 (REPORT.md:14)
 METRIC = "zone-updates/s"
 
@@ -44,20 +50,40 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--scheme", default="unsplit", choices=["unsplit", "ct", "march1d"],
+                    help="unsplit GLM step (the headline), constrained transport, or the march scheme")
     ap.add_argument("--recon", default="mc")
-    ap.add_argument("--riemann", default="hlld")
+    ap.add_argument("--riemann", default=None, help="default: hlld (unsplit, ct), hll (march1d)")
+    ap.add_argument("--emf", default="contact", choices=["contact", "average"], help="CT edge EMF")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--tile", default="", help="force tile as X,Y,Z")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.riemann is None:
+        a.riemann = "hll" if a.scheme == "march1d" else "hlld"
+    return a
+
+
+def nvar(args):
+    return 8 if args.scheme == "ct" else 9
 
 
 def workload_config(args, extra=None):
-    c = {"workload": f"glm_mhd_{args.n}^3_{args.dtype}_plm_{args.riemann}_glm_forcing", "n": args.n,
-         "scheme": "unsplit", "recon": args.recon, "riemann": args.riemann, "forcing": "ou_61_modes",
+    recon = "ppm" if args.recon == "ppm" else "plm"
+    if args.scheme == "ct":
+        name = f"ct_mhd_{args.n}^3_{args.dtype}_{recon}_{args.riemann}_{args.emf}_emf_forcing"
+    elif args.scheme == "march1d":
+        name = f"march_mhd_{args.n}^3_{args.dtype}_{recon}_hll_glm"
+    else:
+        name = f"glm_mhd_{args.n}^3_{args.dtype}_{recon}_{args.riemann}_glm_forcing"
+    c = {"workload": name, "n": args.n, "scheme": args.scheme, "recon": args.recon, "riemann": args.riemann,
+         "forcing": "none" if args.scheme == "march1d" else "ou_61_modes",
          "gamma": GAMMA, "courant": COURANT, "ic": "seeded synthetic turbulence, Mach 1, seed 1",
-         "l2": "inputs larger than L2 (state %.2f GB per register)" % (args.n ** 3 * 9 * (4 if args.dtype == "f32" else 8) / 1e9)}
+         "l2": "inputs larger than L2 (state %.2f GB per register)"
+               % (args.n ** 3 * nvar(args) * (4 if args.dtype == "f32" else 8) / 1e9)}
+    if args.scheme == "ct":
+        c["emf"] = args.emf
     if extra:
         c.update(extra)
     return c
@@ -124,31 +150,44 @@ def ncu_traffic(args):
     """DRAM bytes per zone of the step kernel from the committed ncu summary (profiles/)."""
     try:
         t = json.load(open(os.path.join(ROOT, "profiles", "step_kernel_traffic.json")))
-        key = f"unsplit_{args.dtype}_{args.recon}_{args.riemann}"
+        key = f"{args.scheme}_{args.dtype}_{args.recon}_{args.riemann}"
         return t[key]["dram_bytes_per_zone"], t[key].get("note", "")
     except Exception:
         return None, ""
 
 
 # --------------------------------------------------------------------------------------------
-def cpu_baseline_sample(dtype, recon, riemann, target_s=12.0):
+def oracle_sample(O, args, n, np_dtype):
+    """(config, state, step(u, dt, ch, fac, ramp, modes)) of the oracle for the bench's scheme."""
+    import numpy as np
+    cfg = O.Config(n=(n, n, n), gamma=GAMMA, recon=args.recon, riemann=args.riemann, iflo=True,
+                   emf=args.emf if args.scheme == "ct" else "average")
+    if args.scheme == "ct":
+        u = O.ct_ic_ot(cfg).astype(np_dtype)
+        return cfg, u, lambda u, dt, ch, fac, ramp, modes: O.ct_step(cfg, u, dt, ramp, modes)
+    u = O.ic_uniform(cfg, 1.0, 0.6, (0.775, 0.0, 0.0)).astype(np_dtype)
+    rng = np.random.default_rng(1)
+    u[1:4] += (0.5 * rng.standard_normal(u[1:4].shape)).astype(np_dtype)
+    if args.scheme == "march1d":
+        return cfg, u, lambda u, dt, ch, fac, ramp, modes: O.step_march1d(cfg, u, dt, ch, fac)
+    return cfg, u, lambda u, dt, ch, fac, ramp, modes: O.step_unsplit(cfg, u, dt, ch, fac, ramp, modes)
+
+
+def cpu_baseline_sample(args, target_s=12.0):
     """Oracle (C++ restatement, all host threads) on a bounded sample of the same scheme."""
     import numpy as np
     from oracle import oracle as O
     nthr = O.set_threads(os.cpu_count() or 1)
-    np_dtype = np.float32 if dtype == "f32" else np.float64
+    np_dtype = np.float32 if args.dtype == "f32" else np.float64
 
     def run(n, steps):
-        cfg = O.Config(n=(n, n, n), gamma=GAMMA, recon=recon, riemann=riemann, iflo=True)
-        u = O.ic_uniform(cfg, 1.0, 0.6, (0.775, 0.0, 0.0)).astype(np_dtype)
-        rng = np.random.default_rng(1)
-        u[1:4] += (0.5 * rng.standard_normal(u[1:4].shape)).astype(np_dtype)
+        cfg, u, step = oracle_sample(O, args, n, np_dtype)
         f = O.OUForcing(amp=AMP, T=0.5, seed=1)
         f.advance()
         dt = 1e-4
         t0 = time.perf_counter()
         for _ in range(steps):
-            u = O.step_unsplit(cfg, u, dt, 2.0, 0.99, 0.5, f.modes)
+            u = step(u, dt, 2.0, 0.99, 0.5, f.modes)
         return time.perf_counter() - t0
 
     t32 = run(32, 1)
@@ -160,8 +199,8 @@ def cpu_baseline_sample(dtype, recon, riemann, target_s=12.0):
     steps = max(1, min(4, int(target_s / (per_zone * n ** 3))))
     el = run(n, steps)
     return {"value": n ** 3 * steps / el, "unit": METRIC, "cores": nthr, "kind": "port",
-            "sample": f"{steps} step(s) of the same scheme (PLM-{recon}+{riemann}+GLM+forcing, {dtype}) at {n}^3 "
-                      f"with the C++ oracle on {nthr} host threads"}
+            "sample": f"{steps} step(s) of the same scheme ({args.scheme}, {args.recon}+{args.riemann}, {args.dtype}) "
+                      f"at {n}^3 with the C++ oracle on {nthr} host threads"}
 
 
 # --------------------------------------------------------------------------------------------
@@ -174,30 +213,30 @@ def run_reference(args):
     nthr = O.set_threads(os.cpu_count() or 1)
     np_dtype = np.float32 if args.dtype == "f32" else np.float64
     # size one step of the sample to ~2 s so that K + W steps end within a few minutes
-    cfg32 = O.Config(n=(32, 32, 32), gamma=GAMMA, recon=args.recon, riemann=args.riemann)
-    u = O.ic_uniform(cfg32).astype(np_dtype)
+    cfg32, u32, step32 = oracle_sample(O, args, 32, np_dtype)
     t0 = time.perf_counter()
-    O.step_unsplit(cfg32, u, 1e-4, 2.0, 0.99)
+    step32(u32, 1e-4, 2.0, 0.99, 0.0, None)
     per_zone = (time.perf_counter() - t0) / 32 ** 3
     n = 32
     for cand in (48, 64, 80, 96, 112, 128, 160, 192):
         if per_zone * cand ** 3 <= 2.0:
             n = cand
-    cfg = O.Config(n=(n, n, n), gamma=GAMMA, recon=args.recon, riemann=args.riemann, iflo=True)
-    u = O.ic_uniform(cfg, 1.0, 0.6, (0.775, 0.0, 0.0)).astype(np_dtype)
-    rng = np.random.default_rng(1)
-    u[1:4] += (0.5 * rng.standard_normal(u[1:4].shape)).astype(np_dtype)
+    cfg, u, one = oracle_sample(O, args, n, np_dtype)
+    cflf = O.ct_cfl if args.scheme == "ct" else O.cfl
     f = O.OUForcing(amp=AMP, T=0.5, seed=1)
     f.advance()
     t = 0.0
+    forcing = args.scheme != "march1d"
 
     def step(u, t):
-        while t >= f.next_time:
+        while forcing and t >= f.next_time:
             f.advance()
-        cmax, smax = O.cfl(cfg, u)
-        dt = min(COURANT * cfg.dx / cmax, f.next_time - t)
+        cmax, smax = cflf(cfg, u)
+        dt = COURANT * cfg.dx / cmax
+        if forcing:
+            dt = min(dt, f.next_time - t)
         fac = math.exp(-(smax / CP_COEF) * dt)
-        return O.step_unsplit(cfg, u, dt, smax, fac, min(t / 0.5, 1.0), f.modes), t + dt
+        return one(u, dt, smax, fac, min(t / 0.5, 1.0), f.modes if forcing else None), t + dt
 
     for _ in range(args.warmup):
         u, t = step(u, t)
@@ -213,7 +252,7 @@ def run_reference(args):
            "config": workload_config(args, {"sample_n": n}),
            "cpu_baseline": {"value": value, "unit": METRIC, "cores": nthr, "kind": "port",
                             "sample": f"each step = one step of the same scheme at {n}^3 (CFL + forcing + "
-                                      f"PLM-{args.recon}+{args.riemann}+GLM) with the C++ oracle"},
+                                      f"{args.scheme} {args.recon}+{args.riemann}) with the C++ oracle"},
            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
@@ -236,14 +275,14 @@ def run_ours(args):
     # the CPU baseline runs before any GPU work of this process (OpenMP threads, no fork)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline_sample(args.dtype, args.recon, args.riemann)
+        cpu = cpu_baseline_sample(args)
 
     from glmmhdturb_b200 import Solver, autotune
     n = args.n
     tile, tuned = (0, 0, 0), None
     if args.tile:
         tile = tuple(int(v) for v in args.tile.split(","))
-    elif not args.no_tune:
+    elif not args.no_tune and args.scheme == "unsplit":
         c = autotune.cached(n, args.dtype, "unsplit", args.recon, args.riemann)
         if c:
             tile, tuned = tuple(c["tile"]), {"source": "cache", "ms": c["ms"]}
@@ -251,8 +290,9 @@ def run_ours(args):
             tile, ms, res = autotune.tune(n, dtype=args.dtype, recon=args.recon, riemann=args.riemann)
             tuned = {"source": "autotune", "ms": ms, "candidates": len(res),
                      "top": [[list(t), round(m, 3)] for m, t in res[:6]]}
-    s = Solver(n, dtype=args.dtype, recon=args.recon, riemann=args.riemann, gamma=GAMMA, courant=COURANT,
-               turb_amp=AMP, turb_T=0.5, turb_ndt=100, turb_seed=1, tile=tile)
+    s = Solver(n, dtype=args.dtype, scheme=args.scheme, recon=args.recon, riemann=args.riemann, emf=args.emf,
+               gamma=GAMMA, courant=COURANT, turb_amp=AMP, turb_T=0.5, turb_ndt=100, turb_seed=1, tile=tile)
+    forcing = args.scheme != "march1d"
     stream = torch.cuda.current_stream()
     u = s.alloc()
     w = s.alloc()
@@ -271,21 +311,23 @@ def run_ours(args):
 
     def one_step(record):
         nonlocal u, w
-        while st["t"] >= s.next_time:
+        while forcing and st["t"] >= s.next_time:
             s.forcing_advance()
             st["launches"] += 2          # OU update + mode-table refresh
-        dt = min(COURANT * s.dx / st["cm"], s.next_time - st["t"])
+        dt = COURANT * s.dx / st["cm"]
+        if forcing:
+            dt = min(dt, s.next_time - st["t"])
         ch = st["sm"]
         fac = math.exp(-(ch / CP_COEF) * dt)
         if record:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-        s.step(u, w, dt, t=st["t"], ch=ch, glm_fac=fac, do_turb=True, want_cfl=True)
+        s.step(u, w, dt, t=st["t"], ch=ch, glm_fac=fac, do_turb=forcing, want_cfl=True)
         if record:
             e1.record(stream)
             kernel_events.append((e0, e1))
-        st["launches"] += 1
+        st["launches"] += STEP_LAUNCHES[args.scheme]
         st["cm"], st["sm"] = s.cfl_result()   # dt of the next step needs this scalar on the host
         u, w = w, u
         st["t"] += dt
@@ -358,14 +400,16 @@ def run_ours(args):
         peak = peaks.get("hbm_gbs")
         peak_src = "measured" if peak else "fallback"
         peak = peak or 6650.0
-        alg = BYTES_PER_ZONE[args.dtype] * zones
+        alg = BYTES_PER_ZONE[args.dtype] * nvar(args) // 9 * zones
         achieved = alg / (kmean * 1e-3) / 1e9
         tb, note = ncu_traffic(args)
         value = world * zones * args.steps / (ms * 1e-3)
         info = s.kernel_info()
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": value / PUBLISHED_A6000, "dtype": args.dtype,
+               "scaling": "weak",
+               "vs_baseline": value / PUBLISHED_A6000 if args.scheme == "unsplit" and args.n == 512 else None,
+               "dtype": args.dtype,
                "data": "synthetic",
                "config": workload_config(args, {"parallelism": f"replicas{world}" if world > 1 else "single",
                                                 "tile": list(info["tile"]), "regs": info["regs"],
@@ -379,7 +423,7 @@ def run_ours(args):
                "gpu_launches": launches,
                "clocks": clk,
                "e2e": e2e,
-               "diagnostics": {k: diag[k] for k in ("vrms", "divbmax", "rhomin", "finite")}}
+               "diagnostics": {k: diag[k] for k in ("vrms", "divbmax", "rhomin", "finite") if k in diag}}
         if cpu is not None:
             out["cpu_baseline"] = cpu
         print(json.dumps(out), flush=True)

@@ -746,7 +746,6 @@ int gmt_ic_uniform(gmt_ctx* c, void* u, double rho0, double p0, double bx0, doub
 int gmt_ic_turbulent(gmt_ctx* c, void* u, double rho0, double p0, double bx0, double by0, double bz0, double mach,
                      double db, uint32_t seed, void* stream) {
     if (!c || !u) return fail(GMT_ERR_ARG, "null argument");
-    if (c->p.scheme == GMT_SCHEME_CT) return fail(GMT_ERR_ARG, "gmt_ic_turbulent: GLM state only");
     if (!(rho0 > 0) || !(p0 > 0)) return fail(GMT_ERR_ARG, "gmt_ic_turbulent: rho0 and p0 must be positive");
     cudaStream_t s = (cudaStream_t)stream;
     double* m = nullptr;
@@ -757,7 +756,16 @@ int gmt_ic_turbulent(gmt_ctx* c, void* u, double rho0, double p0, double bx0, do
     if (e == cudaSuccess) e = launch_ou_update(m, seed, 0u, 0.0, 1.0, forcing_sigma0(1.0, 0.0, 1.0), s);
     const double b0[3] = {bx0, by0, bz0};
     const double vscale = mach * std::sqrt(c->p.gamma * p0 / rho0);
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && c->p.scheme == GMT_SCHEME_CT) {
+        // face fields from an edge vector potential (divergence-free to round-off); the CT scratch
+        // holds the three potential planes
+        e = c->esize == 8 ? launch_ct_ic_turb<double>(planes8<double>(u, c->n), c->p.nx, c->p.ny, c->p.nz, m,
+                                                      static_cast<double*>(c->ct_scratch), rho0, p0, b0, vscale, db,
+                                                      c->p.gamma, s)
+                          : launch_ct_ic_turb<float>(planes8<float>(u, c->n), c->p.nx, c->p.ny, c->p.nz, m,
+                                                     static_cast<float*>(c->ct_scratch), rho0, p0, b0, vscale, db,
+                                                     c->p.gamma, s);
+    } else if (e == cudaSuccess) {
         if (c->esize == 8) {
             e = launch_btab<double>(m, (const double*)c->trig[1], (const double*)c->trig[2], c->p.ny, c->p.nz,
                                     (double*)bt, s);

@@ -367,6 +367,94 @@ cudaError_t launch_ic_turb(const Planes<R>& u, int nx, int ny, int nz, const R* 
     return cudaGetLastError();
 }
 
+// Turbulent CT state: the GLM state's density and velocity (one unit-rms draw a(x) of the 61-mode
+// solenoidal field, evaluated at cell centres by direct mode sum), and face fields
+// B = B0 + curl(A) with A = db / (4 pi) a evaluated on the cell edges.  The discrete curl of an
+// edge potential has zero face divergence to round-off.
+__device__ __forceinline__ void mode_field(const double* modes, double x, double y, double z, double a[3]) {
+    a[0] = a[1] = a[2] = 0.0;
+    const double twopi = 6.283185307179586476925286766559;
+    for (int q = 0; q < NMODES; ++q) {
+        const double ph = twopi * (c_mode_k[3 * q] * x + c_mode_k[3 * q + 1] * y + c_mode_k[3 * q + 2] * z);
+        double sn, cs;
+        sincos(ph, &sn, &cs);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a[c] += 2.0 * (modes[(q * 3 + c) * 2] * cs - modes[(q * 3 + c) * 2 + 1] * sn);
+    }
+}
+
+// pass 1: edge potentials Ax (i, j-1/2, k-1/2), Ay (i-1/2, j, k-1/2), Az (i-1/2, j-1/2, k) of every cell
+template <class R>
+__global__ void ct_turb_edges_kernel(R* ax, R* ay, R* az, int nx, int ny, int nz, const double* modes, double scale) {
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+        const double x = (i + 0.5) / nx, y = (j + 0.5) / ny, z = (k + 0.5) / nz;
+        const double xl = (double)i / nx, yl = (double)j / ny, zl = (double)k / nz;
+        double a[3];
+        mode_field(modes, x, yl, zl, a);
+        ax[c] = (R)(scale * a[0]);
+        mode_field(modes, xl, y, zl, a);
+        ay[c] = (R)(scale * a[1]);
+        mode_field(modes, xl, yl, z, a);
+        az[c] = (R)(scale * a[2]);
+    }
+}
+
+// pass 2: rho, momentum at cell centres and face B = B0 + curl A (lower faces)
+template <class R>
+__global__ void ct_turb_faces_kernel(const Planes8<R> q, const R* ax, const R* ay, const R* az, int nx, int ny, int nz,
+                                     const double* modes, double rho0, double vscale, double b0x, double b0y, double b0z) {
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+        const size_t cyp = (size_t)i + (size_t)nx * (wrapi(j + 1, ny) + (size_t)ny * k);
+        const size_t czp = (size_t)i + (size_t)nx * (j + (size_t)ny * wrapi(k + 1, nz));
+        const size_t cxp = (size_t)wrapi(i + 1, nx) + (size_t)nx * (j + (size_t)ny * k);
+        // Bx(i-1/2, j, k) = dAz/dy - dAy/dz;  By(i, j-1/2, k) = dAx/dz - dAz/dx;  Bz(i, j, k-1/2) = dAy/dx - dAx/dy
+        q.p[5][c] = (R)(b0x + ((double)az[cyp] - (double)az[c]) * ny - ((double)ay[czp] - (double)ay[c]) * nz);
+        q.p[6][c] = (R)(b0y + ((double)ax[czp] - (double)ax[c]) * nz - ((double)az[cxp] - (double)az[c]) * nx);
+        q.p[7][c] = (R)(b0z + ((double)ay[cxp] - (double)ay[c]) * nx - ((double)ax[cyp] - (double)ax[c]) * ny);
+        double a[3];
+        mode_field(modes, (i + 0.5) / nx, (j + 0.5) / ny, (k + 0.5) / nz, a);
+        const double rho = rho0 * exp(0.2 * a[1]);
+        q.p[0][c] = (R)rho;
+        q.p[1][c] = (R)(rho * vscale * a[0]);
+        q.p[2][c] = (R)(rho * vscale * a[1]);
+        q.p[3][c] = (R)(rho * vscale * a[2]);
+    }
+}
+
+// pass 3: total energy with the face-averaged field
+template <class R>
+__global__ void ct_turb_energy_kernel(const Planes8<R> q, int nx, int ny, int nz, double p0, double gamma) {
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+        const size_t cxp = (size_t)wrapi(i + 1, nx) + (size_t)nx * (j + (size_t)ny * k);
+        const size_t cyp = (size_t)i + (size_t)nx * (wrapi(j + 1, ny) + (size_t)ny * k);
+        const size_t czp = (size_t)i + (size_t)nx * (j + (size_t)ny * wrapi(k + 1, nz));
+        const double bx = 0.5 * ((double)q.p[5][c] + (double)q.p[5][cxp]);
+        const double by = 0.5 * ((double)q.p[6][c] + (double)q.p[6][cyp]);
+        const double bz = 0.5 * ((double)q.p[7][c] + (double)q.p[7][czp]);
+        const double rho = q.p[0][c], mx = q.p[1][c], my = q.p[2][c], mz = q.p[3][c];
+        q.p[4][c] = (R)(p0 / (gamma - 1.0) + 0.5 * (mx * mx + my * my + mz * mz) / rho + 0.5 * (bx * bx + by * by + bz * bz));
+    }
+}
+
+template <class R>
+cudaError_t launch_ct_ic_turb(const Planes8<R>& q, int nx, int ny, int nz, const double* modes, R* scratch, double rho0,
+                              double p0, const double b0[3], double vscale, double db, double gamma, cudaStream_t s) {
+    const size_t n = (size_t)nx * ny * nz;
+    const int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    const double scale = db / (4.0 * 3.141592653589793238462643383279);
+    ct_turb_edges_kernel<R><<<nb, 256, 0, s>>>(scratch, scratch + n, scratch + 2 * n, nx, ny, nz, modes, scale);
+    ct_turb_faces_kernel<R><<<nb, 256, 0, s>>>(q, scratch, scratch + n, scratch + 2 * n, nx, ny, nz, modes, rho0, vscale,
+                                               b0[0], b0[1], b0[2]);
+    ct_turb_energy_kernel<R><<<nb, 256, 0, s>>>(q, nx, ny, nz, p0, gamma);
+    return cudaGetLastError();
+}
+
 #define GMT_INST(R)                                                                                              \
     template cudaError_t launch_cfl<R>(const CPlanes<R>&, size_t, const Consts<R>&, unsigned long long*,         \
                                        cudaStream_t);                                                            \
@@ -381,7 +469,9 @@ cudaError_t launch_ic_turb(const Planes<R>& u, int nx, int ny, int nz, const R* 
     template cudaError_t launch_ic_uniform<R>(const Planes<R>&, size_t, const double*, cudaStream_t);            \
     template cudaError_t launch_ic_turb<R>(const Planes<R>&, int, int, int, const R*, const R*, double, double,       \
                                            const double*, double, double, double, cudaStream_t);                 \
-    template cudaError_t launch_ct_ic_ot<R>(const Planes8<R>&, int, int, int, double, cudaStream_t);
+    template cudaError_t launch_ct_ic_ot<R>(const Planes8<R>&, int, int, int, double, cudaStream_t);                \
+    template cudaError_t launch_ct_ic_turb<R>(const Planes8<R>&, int, int, int, const double*, R*, double, double,   \
+                                              const double*, double, double, double, cudaStream_t);
 GMT_INST(float)
 GMT_INST(double)
 

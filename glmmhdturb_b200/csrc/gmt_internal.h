@@ -85,6 +85,9 @@ template <class R> cudaError_t launch_btab(const double* modes, const R* trigy, 
 template <class R> cudaError_t launch_ic_ot(const Planes<R>& u, int nx, int ny, int nz, double gamma, cudaStream_t s);
 template <class R> cudaError_t launch_ic_uniform(const Planes<R>& u, size_t n, const double v9[9], cudaStream_t s);
 template <class R> cudaError_t launch_ct_ic_ot(const Planes8<R>& q, int nx, int ny, int nz, double gamma, cudaStream_t s);
+template <class R> cudaError_t launch_ct_ic_turb(const Planes8<R>& q, int nx, int ny, int nz, const double* modes,
+                                                 R* scratch, double rho0, double p0, const double b0[3], double vscale,
+                                                 double db, double gamma, cudaStream_t s);
 template <class R> cudaError_t launch_ic_turb(const Planes<R>& u, int nx, int ny, int nz, const R* btab,
                                              const R* trigx, double rho0, double p0, const double b0[3],
                                              double vscale, double bscale, double gamma, cudaStream_t s);

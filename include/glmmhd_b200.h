@@ -208,7 +208,8 @@ int gmt_ic_uniform(gmt_ctx* ctx, void* u, double rho0, double p0, double bx0, do
                    void* stream);                                          /* glmmhd_turb.jl:2164 */
 /* seeded synthetic turbulent state (stand-in for a pre-evolved checkpoint): the uniform state plus
  * v = mach*c_s*a(x), dB = db*a(x), rho = rho0*exp(0.2 a_y(x)), a = one unit-rms draw of the 61-mode
- * solenoidal field with Philox seed `seed` */
+ * solenoidal field with Philox seed `seed`.  In a CT context the face fields are
+ * B0 + curl(db/(4 pi) a) taken on the cell edges, so the face divergence is zero to round-off. */
 int gmt_ic_turbulent(gmt_ctx* ctx, void* u, double rho0, double p0, double bx0, double by0, double bz0,
                      double mach, double db, uint32_t seed, void* stream);
 
