@@ -76,6 +76,7 @@ struct gmt_ctx {
     void* btab = nullptr;     // [nz][ny][24] reals
     void* trig[3] = {nullptr, nullptr, nullptr};
     void* ct_scratch = nullptr;
+    void* fmass = nullptr;         // march with species: lower-face mass fluxes (3 planes)
     unsigned long long* divb = nullptr;
     int* err = nullptr;       // device flag set by kernels whose bounded waits gave up
     LoopState* loop = nullptr;     // device-resident time loop record (gmt_run)
@@ -175,6 +176,7 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.err = c->err;
         A.dx = (R)dx;
         A.dparams = nullptr;
+        A.fmass = nullptr;
         if (a->want_cfl) {
             GMT_CUDA(cudaMemsetAsync(c->cfl, 0, 2 * sizeof(unsigned long long), s));
             A.cfl_out = c->cfl;
@@ -184,8 +186,10 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         if (e != cudaSuccess) return cuda_fail(e, "unsplit step");
         return GMT_OK;
     }
-    if (p.scheme == GMT_SCHEME_MARCH1D && p.nsp == 0) {
-        // the tiled march: the unsplit tile with the march scheme (one solve per face)
+    if (p.scheme == GMT_SCHEME_MARCH1D) {
+        // the tiled march: the unsplit tile with the march scheme (one solve per face); with
+        // passive species it also stores the face mass fluxes for the species pass
+        if (p.nsp > 0 && (!sp_in || !sp_out)) return fail(GMT_ERR_ARG, "gmt_step: species planes missing");
         UnsplitArgs<R> A;
         A.u = u; A.o = o;
         A.nx = p.nx; A.ny = p.ny; A.nz = p.nz;
@@ -201,38 +205,31 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.err = c->err;
         A.dx = (R)dx;
         A.dparams = nullptr;
+        A.fmass = p.nsp > 0 ? static_cast<R*>(c->fmass) : nullptr;
         if (a->want_cfl) {
             GMT_CUDA(cudaMemsetAsync(c->cfl, 0, 2 * sizeof(unsigned long long), s));
             A.cfl_out = c->cfl;
         }
         cudaError_t e = launch_march_tiled(A, p.recon, s);
         if (e != cudaSuccess) return cuda_fail(e, "march step");
-        return GMT_OK;
-    }
-    if (p.scheme == GMT_SCHEME_MARCH1D) {
-        // with passive species: one thread per cell
-        MarchArgs<R> A;
-        A.u = u; A.o = o;
-        A.nx = p.nx; A.ny = p.ny; A.nz = p.nz;
-        A.ox = c->ox; A.oy = c->oy; A.lz = c->lz;
-        A.dtdx = (R)(a->dt / dx);
-        A.ch = (R)a->ch; A.glm_fac = (R)a->glm_fac;
-        A.K = consts_of<R>(p);
-        A.ppm = p.recon == GMT_RECON_PPM;
-        A.nsp = p.nsp;
-        for (int k = 0; k < MAX_SPECIES; ++k) { A.su[k] = nullptr; A.so[k] = nullptr; }
-        if (p.nsp > 0 && (!sp_in || !sp_out)) return fail(GMT_ERR_ARG, "gmt_step: species planes missing");
-        for (int k = 0; k < p.nsp; ++k) {
-            A.su[k] = static_cast<const R*>(sp_in[k]);
-            A.so[k] = static_cast<R*>(sp_out[k]);
-            if (!A.su[k] || !A.so[k]) return fail(GMT_ERR_ARG, "gmt_step: null species plane");
-        }
-        cudaError_t e = launch_march1d(A, s);
-        if (e != cudaSuccess) return cuda_fail(e, "march1d step");
-        if (a->want_cfl) {
-            e = launch_cfl<R>(CPlanes<R>{{o.p[0], o.p[1], o.p[2], o.p[3], o.p[4], o.p[5], o.p[6], o.p[7], o.p[8]}},
-                              c->n, A.K, c->cfl, s);
-            if (e != cudaSuccess) return cuda_fail(e, "cfl");
+        if (p.nsp > 0) {
+            MarchArgs<R> M;
+            M.u = u; M.o = o;
+            M.nx = p.nx; M.ny = p.ny; M.nz = p.nz;
+            M.ox = c->ox; M.oy = c->oy; M.lz = c->lz;
+            M.dtdx = A.dtdx;
+            M.ch = A.ch; M.glm_fac = A.glm_fac;
+            M.K = A.K;
+            M.ppm = p.recon == GMT_RECON_PPM;
+            M.nsp = p.nsp;
+            for (int k = 0; k < MAX_SPECIES; ++k) { M.su[k] = nullptr; M.so[k] = nullptr; }
+            for (int k = 0; k < p.nsp; ++k) {
+                M.su[k] = static_cast<const R*>(sp_in[k]);
+                M.so[k] = static_cast<R*>(sp_out[k]);
+                if (!M.su[k] || !M.so[k]) return fail(GMT_ERR_ARG, "gmt_step: null species plane");
+            }
+            e = launch_species(M, static_cast<const R*>(c->fmass), s);
+            if (e != cudaSuccess) return cuda_fail(e, "species step");
         }
         return GMT_OK;
     }
@@ -360,7 +357,7 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     c->n = (size_t)p->nx * p->ny * p->nz;
     cudaGetDevice(&c->device);
     int rc = GMT_OK;
-    if (p->scheme == GMT_SCHEME_UNSPLIT || (p->scheme == GMT_SCHEME_MARCH1D && p->nsp == 0)) rc = choose_tile(c);
+    if (p->scheme == GMT_SCHEME_UNSPLIT || p->scheme == GMT_SCHEME_MARCH1D) rc = choose_tile(c);
     if (p->scheme == GMT_SCHEME_CT) rc = choose_tile(c, true);
     if (rc != GMT_OK) { delete c; return rc; }
     auto alloc = [&](void** ptr, size_t bytes) -> bool {
@@ -376,6 +373,7 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     const int dims[3] = {p->nx, p->ny, p->nz};
     for (int a = 0; ok && a < 3; ++a) ok = alloc(&c->trig[a], (size_t)8 * dims[a] * c->esize);
     if (ok && p->scheme == GMT_SCHEME_CT) ok = alloc(&c->ct_scratch, (size_t)15 * c->n * c->esize);
+    if (ok && p->scheme == GMT_SCHEME_MARCH1D && p->nsp > 0) ok = alloc(&c->fmass, (size_t)3 * c->n * c->esize);
     if (ok) ok = alloc((void**)&c->divb, sizeof(unsigned long long));
     if (ok) ok = alloc((void**)&c->err, sizeof(int));
     if (ok) ok = alloc((void**)&c->loop, sizeof(LoopState)) && alloc((void**)&c->loopc, sizeof(LoopConst)) &&
@@ -431,6 +429,7 @@ int gmt_destroy(gmt_ctx* c) {
     cudaFree(c->btab);
     for (auto& t : c->trig) cudaFree(t);
     cudaFree(c->ct_scratch);
+    cudaFree(c->fmass);
     cudaFree(c->divb);
     cudaFree(c->err);
     for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
@@ -454,13 +453,9 @@ int gmt_kernel_info(gmt_ctx* c, int32_t* regs, int64_t* smem, int32_t tile[3]) {
                          c->ox * c->oy);
         sm = (int64_t)unsplit_smem(c->esize, c->ox, c->oy);
     } else if (c->p.scheme == GMT_SCHEME_MARCH1D) {
-        if (c->p.nsp > 0) {
-            r = march1d_regs(c->esize);
-        } else {
-            r = c->esize == 8 ? march_tiled_regs((const UnsplitArgs<double>*)nullptr, c->p.recon, c->ox * c->oy)
-                              : march_tiled_regs((const UnsplitArgs<float>*)nullptr, c->p.recon, c->ox * c->oy);
-            sm = (int64_t)unsplit_smem(c->esize, c->ox, c->oy);
-        }
+        r = c->esize == 8 ? march_tiled_regs((const UnsplitArgs<double>*)nullptr, c->p.recon, c->ox * c->oy)
+                          : march_tiled_regs((const UnsplitArgs<float>*)nullptr, c->p.recon, c->ox * c->oy);
+        sm = (int64_t)unsplit_smem(c->esize, c->ox, c->oy);
     } else {
         r = ct_regs_of(c->esize, c->p.recon, c->p.riemann, c->ox * c->oy);
         sm = (int64_t)ct_smem_of(c->esize, c->ox, c->oy);
@@ -836,6 +831,7 @@ cudaError_t run_enqueue(gmt_ctx* c, const void* src, void* dst, int flags, cudaS
     A.err = c->err;
     A.dx = (R)(p.boxlen / p.nx);
     A.dparams = reinterpret_cast<const double*>(c->loop);
+    A.fmass = nullptr;
     int riem = p.riemann == GMT_RIEMANN_LLF ? GMT_RIEMANN_HLLD : p.riemann;
     return launch_unsplit(A, p.recon, riem, s);
 }
@@ -970,6 +966,7 @@ template <class R> int ens_bind(gmt_ensemble* E, void* const* u, void* const* w,
             a.err = E->err;
             a.dx = (R)(E->p.boxlen / n);
             a.dparams = reinterpret_cast<const double*>(E->loop + b);
+            a.fmass = nullptr;
         }
     cudaError_t e = cudaMemcpy(E->args, A.data(), A.size() * sizeof(UnsplitArgs<R>), cudaMemcpyHostToDevice);
     return e == cudaSuccess ? GMT_OK : cuda_fail(e, "ensemble bind");

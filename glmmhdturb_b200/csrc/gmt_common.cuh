@@ -33,6 +33,8 @@ template <class R> struct UnsplitArgs {
     int* err;              // set to 1 when a bounded wait gives up (never expected)
     R dx;                  // cell size (dt/dx of device-supplied steps)
     const double* dparams; // if set: dt, ch, glm_fac, ramp of this step read from device memory
+    R* fmass;              // if set: the mass fluxes of every cell's lower x, y, z faces (3 planes),
+                           // for the passive-species pass of the march scheme
 };
 
 // step values of one box, from the kernel arguments or from device memory

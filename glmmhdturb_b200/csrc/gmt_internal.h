@@ -32,7 +32,7 @@ int unsplit_regs(int dtype_bytes, int recon, int riem, int nthreads);
 
 // transverse-free 1-D Hancock march (gmt_march1d.cu)
 constexpr int MAX_SPECIES = 8;
-template <class R> struct MarchArgs {
+template <class R> struct MarchArgs {   // the species pass of the march scheme
     CPlanes<R> u;
     Planes<R> o;
     int nx, ny, nz, ox, oy, lz;
@@ -43,9 +43,9 @@ template <class R> struct MarchArgs {
     const R* su[MAX_SPECIES];
     R* so[MAX_SPECIES];
 };
-cudaError_t launch_march1d(const MarchArgs<float>& A, cudaStream_t s);
-cudaError_t launch_march1d(const MarchArgs<double>& A, cudaStream_t s);
-int march1d_regs(int dtype_bytes);
+// passive species of the march scheme, after the tiled step stored the face mass fluxes
+cudaError_t launch_species(const MarchArgs<float>& A, const float* fmass, cudaStream_t s);
+cudaError_t launch_species(const MarchArgs<double>& A, const double* fmass, cudaStream_t s);
 
 // constrained transport (gmt_ct.cu): q = [rho, mx, my, mz, E, bxf, byf, bzf]
 template <class R> struct CTArgs {

@@ -291,10 +291,15 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
         }
         {
             Q9<R> XY;
+            R fmx = R(0), fmy = R(0);   // lower-face mass fluxes, kept when A.fmass is set
             if (kr - 1 >= z0) {
 #pragma unroll
                 for (int v = 0; v < 9; ++v)
                     XY.v[v] = (ST[(1 * 9 + v) * RN + rown] - Fxh.v[v]) + (ST[(3 * 9 + v) * RN + rown] - Fyh.v[v]);
+                if (A.fmass) {
+                    fmx = ST[(1 * 9 + 0) * RN + rown];
+                    fmy = ST[(3 * 9 + 0) * RN + rown];
+                }
             }
             typename S::Cell r;
             S::recon(PR, PN, PW, cown, s0, sm, sp, K, dtdx, r);
@@ -322,6 +327,12 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
                     S::finish(q, K, V.glm_fac, turb, ax, ay, az, V.dt);
 #pragma unroll
                     for (int v = 0; v < 9; ++v) A.o.p[v][g] = q.v[v];
+                    if (A.fmass) {
+                        const size_t nc = (size_t)nx * ny * nz;
+                        A.fmass[g] = fmx;
+                        A.fmass[nc + g] = fmy;
+                        A.fmass[2 * nc + g] = Fzlo.v[0];
+                    }
                     if (A.cfl_out) {
                         R ct, sg;
                         cfl_speeds(q, K, ct, sg);
