@@ -282,12 +282,14 @@ def run_ours(args):
     tile, tuned = (0, 0, 0), None
     if args.tile:
         tile = tuple(int(v) for v in args.tile.split(","))
-    elif not args.no_tune and args.scheme == "unsplit":
-        c = autotune.cached(n, args.dtype, "unsplit", args.recon, args.riemann)
+    elif not args.no_tune:
+        c = autotune.cached(n, args.dtype, args.scheme, args.recon, args.riemann)
         if c:
             tile, tuned = tuple(c["tile"]), {"source": "cache", "ms": c["ms"]}
         else:
-            tile, ms, res = autotune.tune(n, dtype=args.dtype, recon=args.recon, riemann=args.riemann)
+            kw = {"emf": args.emf} if args.scheme == "ct" else {}
+            tile, ms, res = autotune.tune(n, dtype=args.dtype, scheme=args.scheme, recon=args.recon,
+                                          riemann=args.riemann, **kw)
             tuned = {"source": "autotune", "ms": ms, "candidates": len(res),
                      "top": [[list(t), round(m, 3)] for m, t in res[:6]]}
     s = Solver(n, dtype=args.dtype, scheme=args.scheme, recon=args.recon, riemann=args.riemann, emf=args.emf,

@@ -1,4 +1,5 @@
-"""Autotuner of the step kernel's launch shape: tile (x, y), threads per block and z-chunk length.
+"""Autotuner of the step kernel's launch shape: tile (x, y), threads per block and z-chunk length,
+for the unsplit GLM step, the march scheme and the constrained-transport step.
 
 Each candidate is a separate context (the tile is fixed at gmt_create); candidates are timed with
 CUDA events on the caller's state, best-of-`reps`, and the winner is cached in a JSON file keyed
@@ -40,13 +41,14 @@ def cached(n, dtype="f32", scheme="unsplit", recon="mc", riemann="hlld"):
     return load_cache().get(_key(n, dtype, scheme, recon, riemann))
 
 
-def tune(n, *, dtype="f32", recon="mc", riemann="hlld", gamma=5.0 / 3.0, reps=3, steps=2, tiles=None, chunks=None,
-         save=True, log=None, **solver_kw):
+def tune(n, *, dtype="f32", scheme="unsplit", recon="mc", riemann="hlld", gamma=5.0 / 3.0, reps=3, steps=2,
+         tiles=None, chunks=None, save=True, log=None, **solver_kw):
     """Time every (tile, chunk) candidate on a seeded turbulent state; return the best tile tuple."""
     if isinstance(n, int):
         n = (n, n, n)
     tiles = tiles or TILES[dtype]
     chunks = chunks or CHUNKS
+    solver_kw = dict(solver_kw, scheme=scheme)
     probe = Solver(n, dtype=dtype, recon=recon, riemann=riemann, gamma=gamma, **solver_kw)
     u = probe.alloc()
     w = probe.alloc()
@@ -84,7 +86,7 @@ def tune(n, *, dtype="f32", recon="mc", riemann="hlld", gamma=5.0 / 3.0, reps=3,
     best_ms, best_tile = results[0]
     if save:
         c = load_cache()
-        c[_key(n, dtype, "unsplit", recon, riemann)] = {"tile": list(best_tile), "ms": best_ms,
+        c[_key(n, dtype, scheme, recon, riemann)] = {"tile": list(best_tile), "ms": best_ms,
                                                        "candidates": [[list(t), ms] for ms, t in results]}
         try:
             json.dump(c, open(CACHE, "w"), indent=1)

@@ -108,3 +108,16 @@ def test_kernel_info_reports_resources():
     from glmmhdturb_b200 import Solver
     info = Solver(64, dtype="f32").kernel_info()
     assert 0 < info["regs"] <= 255 and info["smem"] > 0 and info["tile"][0] * info["tile"][1] <= 512
+
+
+@pytest.mark.parametrize("scheme,riemann", [("unsplit", "hlld"), ("march1d", "hll"), ("ct", "hlld")])
+def test_autotuner_picks_a_valid_tile(tmp_path, monkeypatch, scheme, riemann):
+    """The autotuner times tile x z-chunk candidates of each scheme, returns the fastest and caches it."""
+    from glmmhdturb_b200 import autotune
+    monkeypatch.setattr(autotune, "CACHE", str(tmp_path / "tune.json"))
+    tile, ms, res = autotune.tune(32, dtype="f32", scheme=scheme, riemann=riemann, tiles=[(16, 8), (32, 8)],
+                                  chunks=[16, 0], reps=1, steps=1)
+    assert len(res) >= 2 and ms == min(r[0] for r in res) and ms > 0
+    assert tile[0] in (16, 32) and tile[1] == 8
+    c = autotune.cached(32, "f32", scheme, "mc", riemann)
+    assert c and tuple(c["tile"]) == tuple(tile)
