@@ -259,6 +259,22 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------------------------------
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The slowest rank's value (replicas: the job ends when the last box does)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, zones: int, steps: int, ms: float) -> float:
+    """Whole-job zone-updates/s: every rank advances its own box of `zones` cells."""
+    return world * zones * steps / (ms * 1e-3)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -360,10 +376,7 @@ def run_ours(args):
     launches = st["launches"]
     kms = [a.elapsed_time(b) for a, b in kernel_events]
     kmean = sum(kms) / len(kms)
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, world, "cuda")
     diag = s.diagnostics(u)
 
     # ---------------- end to end through the public API from pinned host memory
@@ -386,12 +399,8 @@ def run_ours(args):
         x1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ems = x0.elapsed_time(x1)
-        if world > 1:
-            tt = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ems = float(tt.item())
-        e2e = {"value": world * zones * args.steps / (ems * 1e-3), "unit": METRIC,
+        ems = max_over_ranks(x0.elapsed_time(x1), world, "cuda")
+        e2e = {"value": aggregate_rate(world, zones, args.steps, ems), "unit": METRIC,
                "h2d_bytes_per_step": state_bytes / args.steps,
                "d2h_bytes_per_step": state_bytes / args.steps + 16,
                "note": "initial state uploaded from pinned host memory, K steps with the per-step CFL "
@@ -405,7 +414,7 @@ def run_ours(args):
         alg = BYTES_PER_ZONE[args.dtype] * nvar(args) // 9 * zones
         achieved = alg / (kmean * 1e-3) / 1e9
         tb, note = ncu_traffic(args)
-        value = world * zones * args.steps / (ms * 1e-3)
+        value = aggregate_rate(world, zones, args.steps, ms)
         info = s.kernel_info()
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
