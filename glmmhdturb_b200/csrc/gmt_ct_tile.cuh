@@ -328,10 +328,10 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
     if (tid == 0) mbar_inval(mbar);
 }
 
-template <class R, int RECON, int RIEM, int MAXT, int MINB>
+template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0>
 __global__ void __launch_bounds__(MAXT, MINB) ct_tile_kernel(const CTArgs<R> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    ct_tile<R, RECON, RIEM, 0, 0>(A, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+    ct_tile<R, RECON, RIEM, TOX, TOY>(A, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 template <class R> __device__ __forceinline__ R ct_upwind(R flux, R minus, R plus) {
@@ -406,9 +406,9 @@ template <class R> __global__ void __launch_bounds__(256) ct_face_kernel(const C
 }
 
 // launch: pass A (tile kernel), then B1 and B2; nt <= 0 in A configures the kernel only
-template <class R, int RECON, int RIEM, int MAXT, int MINB>
+template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0>
 static cudaError_t ct_go(const CTArgs<R>& A, cudaStream_t s, bool configure_only) {
-    auto k = ct_tile_kernel<R, RECON, RIEM, MAXT, MINB>;
+    auto k = ct_tile_kernel<R, RECON, RIEM, MAXT, MINB, TOX, TOY>;
     static int configured[64] = {0};
     {
         cudaError_t e = configure_once(k, configured);

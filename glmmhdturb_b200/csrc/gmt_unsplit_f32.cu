@@ -43,9 +43,14 @@ cudaError_t unsplit_prepare_f32() {
         e = march_dispatch_t<float, 512, 1>(none, rc ? RECON_PPM : RECON_MC, 0, true);
         if (e == cudaSuccess) e = march_dispatch_t<float, 256, 2>(none, rc ? RECON_PPM : RECON_MC, 0, true);
     }
+    if (e == cudaSuccess) e = march_go<float, RECON_MC, 512, 1, 32, 16>(none, 0, true);
+    if (e == cudaSuccess) e = march_go<float, RECON_PPM, 512, 1, 32, 16>(none, 0, true);
     return e;
 }
 cudaError_t launch_march_tiled(const UnsplitArgs<float>& A, int recon, cudaStream_t s) {
+    if (A.ox == 32 && A.oy == 16)   // compile-time tile of the production shape
+        return recon == RECON_PPM ? march_go<float, RECON_PPM, 512, 1, 32, 16>(A, s, false)
+                                  : march_go<float, RECON_MC, 512, 1, 32, 16>(A, s, false);
     if (A.ox * A.oy > 256) return march_dispatch_t<float, 512, 1>(A, recon, s, false);
     return march_dispatch_t<float, 256, 2>(A, recon, s, false);
 }

@@ -112,9 +112,9 @@ static cudaError_t ensemble_go(const UnsplitArgs<R>* boxes, const EnsItem* items
 namespace gmt {
 // tiled march launcher (recon MC or PPM; the march has no minmod variant, spike_mhd.cu:118-123);
 // nt <= 0 configures the kernel only
-template <class R, int RECON, int MAXT, int MINB>
+template <class R, int RECON, int MAXT, int MINB, int TOX = 0, int TOY = 0>
 static cudaError_t march_go(const UnsplitArgs<R>& A, cudaStream_t s, bool configure_only) {
-    auto k = march_tile_kernel<R, RECON, MAXT, MINB>;
+    auto k = march_tile_kernel<R, RECON, MAXT, MINB, TOX, TOY>;
     static int configured[64] = {0};
     {
         cudaError_t e = configure_once(k, configured);
