@@ -398,17 +398,30 @@ template <class R> GMT_HD void adj_gather_cell(const AdjArgs<R>& A, size_t c) {
     cell_xyz(A, c, x, y, z);
     const size_t cp[3] = {I.at(x + 1, y, z), I.at(x, y + 1, z), I.at(x, y, z + 1)};
     const size_t cm[3] = {I.at(x - 1, y, z), I.at(x, y - 1, z), I.at(x, y, z - 1)};
+    // all 63 scratch loads (and the 9 state loads) are issued before any use, so a thread keeps
+    // them in flight together: the pass is bound by memory latency, not by arithmetic
+    const R* __restrict__ QB = A.QB;
+    R own[9], ap[27], bm[27];
+#pragma unroll
+    for (int v = 0; v < 9; ++v) own[v] = QB[(size_t)v * I.n + c];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            ap[9 * d + v] = QB[(size_t)(9 + 9 * d + v) * I.n + cp[d]];
+            bm[9 * d + v] = QB[(size_t)(36 + 9 * d + v) * I.n + cm[d]];
+        }
+    const Q9<R> u0 = load_u(A.u, c);
     Q9<R> qb;
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
-        R s = A.QB[(size_t)v * I.n + c];
+        R s = own[v];
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
-            s += -A.QB[(size_t)(9 + 9 * d + v) * I.n + cp[d]] + A.QB[(size_t)(36 + 9 * d + v) * I.n + cm[d]];
+        for (int d = 0; d < 3; ++d) s += -ap[9 * d + v] + bm[9 * d + v];
         qb.v[v] = s;
     }
     Q9<R> ubq = q9_zero<R>();
-    cons2prim_adj(load_u(A.u, c), A.K.gamma, A.K.smallr, A.K.pfl, qb, ubq);
+    cons2prim_adj(u0, A.K.gamma, A.K.smallr, A.K.pfl, qb, ubq);
 #pragma unroll
     for (int v = 0; v < 9; ++v) A.ub.p[v][c] += ubq.v[v];
 }

@@ -32,11 +32,11 @@ template <class R> __global__ void __launch_bounds__(128) adj_update_kernel(cons
     }
     if (threadIdx.x == 0 && A.damp) atomicAdd(A.damp, red[0]);
 }
-template <int RIEM, bool DUALS, class R> __global__ void __launch_bounds__(128) adj_riemann_kernel(const AdjArgs<R> A) {
+template <int RIEM, bool DUALS, class R> __global__ void __launch_bounds__(128, 3) adj_riemann_kernel(const AdjArgs<R> A) {
     const size_t n = (size_t)A.nx * A.ny * A.nz;
     GMT_ADJ_LOOP adj_riemann_cell<RIEM, DUALS>(A, c);
 }
-template <class R> __global__ void __launch_bounds__(128) adj_recon_kernel(const AdjArgs<R> A) {
+template <class R> __global__ void __launch_bounds__(128, 3) adj_recon_kernel(const AdjArgs<R> A) {
     const size_t n = (size_t)A.nx * A.ny * A.nz;
     GMT_ADJ_LOOP adj_recon_cell(A, c);
 }
