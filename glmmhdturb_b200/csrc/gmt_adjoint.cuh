@@ -45,8 +45,10 @@ template <class R> GMT_HD Q9<R> q9_zero() {
 template <class R> struct Idx {
     int nx, ny, nz;
     size_t n;
+    // periodic index of (x, y, z), each coordinate at most one cell outside the box
+    GMT_HD static int wrap1(int i, int m) { return i < 0 ? i + m : (i >= m ? i - m : i); }
     GMT_HD size_t at(int x, int y, int z) const {
-        return (size_t)wrapi(x, nx) + (size_t)nx * ((size_t)wrapi(y, ny) + (size_t)ny * wrapi(z, nz));
+        return (size_t)wrap1(x, nx) + (size_t)nx * ((size_t)wrap1(y, ny) + (size_t)ny * wrap1(z, nz));
     }
 };
 
@@ -64,16 +66,26 @@ template <class R> struct CellRec {
     bool bad[6];      // the face state reverted to m0
 };
 
-template <class R>
-GMT_HD void cell_rec(const CPlanes<R>& u, const Idx<R>& I, int x, int y, int z, const Consts<R>& K,
-                                         R dtdx, int iflo, bool mm, CellRec<R>& r) {
-    r.m0 = cons2prim(load_u(u, I.at(x, y, z)), K.gamma, K.smallr, K.pfl);
-    r.L[0] = cons2prim(load_u(u, I.at(x - 1, y, z)), K.gamma, K.smallr, K.pfl);
-    r.Rr[0] = cons2prim(load_u(u, I.at(x + 1, y, z)), K.gamma, K.smallr, K.pfl);
-    r.L[1] = cons2prim(load_u(u, I.at(x, y - 1, z)), K.gamma, K.smallr, K.pfl);
-    r.Rr[1] = cons2prim(load_u(u, I.at(x, y + 1, z)), K.gamma, K.smallr, K.pfl);
-    r.L[2] = cons2prim(load_u(u, I.at(x, y, z - 1)), K.gamma, K.smallr, K.pfl);
-    r.Rr[2] = cons2prim(load_u(u, I.at(x, y, z + 1)), K.gamma, K.smallr, K.pfl);
+// the seven cells of the reconstruction stencil of (x, y, z), in the order c, x-, x+, y-, y+, z-, z+
+template <class R> GMT_HD void stencil7(const Idx<R>& I, int x, int y, int z, size_t (&cs)[7]) {
+    cs[0] = I.at(x, y, z);
+    cs[1] = I.at(x - 1, y, z);
+    cs[2] = I.at(x + 1, y, z);
+    cs[3] = I.at(x, y - 1, z);
+    cs[4] = I.at(x, y + 1, z);
+    cs[5] = I.at(x, y, z - 1);
+    cs[6] = I.at(x, y, z + 1);
+}
+
+// reconstruction of one cell from the conserved states of its stencil; U(j) returns stencil cell j
+template <class R, class U>
+GMT_HD void cell_rec_from(const U& u, const Consts<R>& K, R dtdx, bool mm, CellRec<R>& r) {
+    r.m0 = cons2prim(u(0), K.gamma, K.smallr, K.pfl);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        r.L[d] = cons2prim(u(1 + 2 * d), K.gamma, K.smallr, K.pfl);
+        r.Rr[d] = cons2prim(u(2 + 2 * d), K.gamma, K.smallr, K.pfl);
+    }
 #pragma unroll
     for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -85,6 +97,21 @@ GMT_HD void cell_rec(const CPlanes<R>& u, const Idx<R>& I, int x, int y, int z, 
     r.mh = cons2prim(r.uh, K.gamma, K.smallr, K.pfl);
     r.hrev = r.mh.v[0] <= K.smallr || r.mh.v[4] <= K.pfl;
     if (r.hrev) r.mh = r.m0;
+}
+
+// stencil source reading the conserved planes
+template <class R> struct StencilGlobal {
+    const CPlanes<R>& u;
+    size_t cs[7];
+    GMT_HD Q9<R> operator()(int j) const { return load_u(u, cs[j]); }
+};
+
+template <class R>
+GMT_HD void cell_rec(const CPlanes<R>& u, const Idx<R>& I, int x, int y, int z, const Consts<R>& K,
+                                         R dtdx, int, bool mm, CellRec<R>& r) {
+    StencilGlobal<R> src{u, {}};
+    stencil7(I, x, y, z, src.cs);
+    cell_rec_from(src, K, dtdx, mm, r);
 }
 
 template <class R>
@@ -197,6 +224,14 @@ GMT_HD void riemann_adj(const Q9<R>& L, const Q9<R>& Rr, const Q9<R>& Fb, int d,
 }
 
 template <class R> GMT_HD void cell_xyz(const AdjArgs<R>& A, size_t c, int& x, int& y, int& z) {
+    if (c <= 0xffffffffu) {   // 32-bit divisions for every linear index below 2^32
+        const unsigned cc = (unsigned)c, nx = (unsigned)A.nx, ny = (unsigned)A.ny;
+        const unsigned q = cc / nx;
+        x = (int)(cc - q * nx);
+        y = (int)(q % ny);
+        z = (int)(q / ny);
+        return;
+    }
     x = (int)(c % A.nx);
     y = (int)((c / A.nx) % A.ny);
     z = (int)(c / ((size_t)A.nx * A.ny));
@@ -212,19 +247,22 @@ template <class R> GMT_HD Q9<R> fs_get(const R* FS, size_t n, size_t c, int k) {
 }
 
 // pass 1: the six interface states of cell c
+template <class R> GMT_HD void adj_faces_store(const AdjArgs<R>& A, size_t n, size_t c, const CellRec<R>& r) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        bool bad;
+        Q9<R> f = rec_face(r, k, A.K, A.iflo, bad);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) A.FS[(size_t)(k * 9 + v) * n + c] = f.v[v];
+    }
+}
 template <class R> GMT_HD void adj_faces_cell(const AdjArgs<R>& A, size_t c) {
     const Idx<R> I = idx_of(A);
     int x, y, z;
     cell_xyz(A, c, x, y, z);
     CellRec<R> r;
     cell_rec(A.u, I, x, y, z, A.K, A.dtdx, A.iflo, A.recon == RECON_MINMOD, r);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        bool bad;
-        Q9<R> f = rec_face(r, k, A.K, A.iflo, bad);
-#pragma unroll
-        for (int v = 0; v < 9; ++v) A.FS[(size_t)(k * 9 + v) * I.n + c] = f.v[v];
-    }
+    adj_faces_store(A, I.n, c, r);
 }
 
 // pass 2: the fluxes at the +x, +y, +z faces of cell c
@@ -303,6 +341,18 @@ template <class R> GMT_HD double adj_update_cell(const AdjArgs<R>& A, size_t c) 
 }
 
 // pass 4: adjoint of the Riemann solves at the +x, +y, +z faces of cell c
+// one face c | cp of direction d: its two interface states and the flux adjoint -> FSbar
+template <int RIEM, bool DUALS, class R>
+GMT_HD void adj_riemann_face(const AdjArgs<R>& A, size_t n, size_t c, size_t cp, int d, const Q9<R>& L,
+                             const Q9<R>& Rr, const Q9<R>& Fb, bool ul) {
+    Q9<R> Lb, Rb;
+    riemann_adj<RIEM, DUALS>(L, Rr, Fb, d, A.K, A.ch, ul, Lb, Rb);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+        A.FSb[(size_t)((2 * d) * 9 + v) * n + c] = Lb.v[v];
+        A.FSb[(size_t)((2 * d + 1) * 9 + v) * n + cp] = Rb.v[v];
+    }
+}
 template <int RIEM, bool DUALS, class R> GMT_HD void adj_riemann_cell(const AdjArgs<R>& A, size_t c) {
     const Idx<R> I = idx_of(A);
     const bool ul = A.use_llf != 0;
@@ -311,27 +361,29 @@ template <int RIEM, bool DUALS, class R> GMT_HD void adj_riemann_cell(const AdjA
 #pragma unroll 1
     for (int d = 0; d < 3; ++d) {
         const size_t cp = d == 0 ? I.at(x + 1, y, z) : (d == 1 ? I.at(x, y + 1, z) : I.at(x, y, z + 1));
-        Q9<R> Fb, Lb, Rb;
+        Q9<R> Fb;
 #pragma unroll
         for (int v = 0; v < 9; ++v) Fb.v[v] = A.dtdx * (A.R1b[(size_t)v * I.n + cp] - A.R1b[(size_t)v * I.n + c]);
-        const Q9<R> L = fs_get(A.FS, I.n, c, 2 * d), Rr = fs_get(A.FS, I.n, cp, 2 * d + 1);
-        riemann_adj<RIEM, DUALS>(L, Rr, Fb, d, A.K, A.ch, ul, Lb, Rb);
-#pragma unroll
-        for (int v = 0; v < 9; ++v) {
-            A.FSb[(size_t)((2 * d) * 9 + v) * I.n + c] = Lb.v[v];
-            A.FSb[(size_t)((2 * d + 1) * 9 + v) * I.n + cp] = Rb.v[v];
-        }
+        adj_riemann_face<RIEM, DUALS>(A, I.n, c, cp, d, fs_get(A.FS, I.n, c, 2 * d), fs_get(A.FS, I.n, cp, 2 * d + 1),
+                                      Fb, ul);
     }
 }
 
 // pass 5: adjoint of the reconstruction of cell c
-template <class R> GMT_HD void adj_recon_cell(const AdjArgs<R>& A, size_t c) {
-    const Idx<R> I = idx_of(A);
+// FSbar source reading the scratch planes
+template <class R> struct FaceBarGlobal {
+    const R* FSb;
+    size_t n, c;
+    GMT_HD Q9<R> operator()(int k) const { return fs_get(FSb, n, c, k); }
+    GMT_HD void release() const {}
+};
+
+// the reconstruction adjoint of cell c from its reconstruction r and the adjoints of its six
+// interface states (FB(k), k = +x, -x, +y, -y, +z, -z); FB(k) is called once per face, in face order,
+// and FB.release() once all six have been read
+template <class R, class FB>
+GMT_HD void adj_recon_core(const AdjArgs<R>& A, size_t n, size_t c, const CellRec<R>& r, const FB& fbar) {
     const bool mm = A.recon == RECON_MINMOD;
-    int x, y, z;
-    cell_xyz(A, c, x, y, z);
-    CellRec<R> r;
-    cell_rec(A.u, I, x, y, z, A.K, A.dtdx, A.iflo, mm, r);
     // faces: f = mh +- s_d, or m0 where reverted
     Q9<R> m0b = q9_zero<R>(), mhb = q9_zero<R>(), sb[3];
 #pragma unroll
@@ -340,7 +392,7 @@ template <class R> GMT_HD void adj_recon_cell(const AdjArgs<R>& A, size_t c) {
     for (int k = 0; k < 6; ++k) {
         bool bad;
         (void)rec_face(r, k, A.K, A.iflo, bad);
-        const Q9<R> fb = fs_get(A.FSb, I.n, c, k);
+        const Q9<R> fb = fbar(k);
         if (bad) {
             q9_add(m0b, fb);
         } else {
@@ -348,6 +400,7 @@ template <class R> GMT_HD void adj_recon_cell(const AdjArgs<R>& A, size_t c) {
             q9_add(sb[k >> 1], fb, (k & 1) ? R(-1) : R(1));
         }
     }
+    fbar.release();   // every interface-state adjoint has been read
     // predictor: mh = c2p(p2c(m0) - h sum_d [F_d(m0 + s_d) - F_d(m0 - s_d)]), or m0 if reverted
     if (r.hrev) {
         q9_add(m0b, mhb);
@@ -384,11 +437,19 @@ template <class R> GMT_HD void adj_recon_cell(const AdjArgs<R>& A, size_t c) {
             slope_deriv(r.m0.v[v] - r.L[d].v[v], r.Rr[d].v[v] - r.m0.v[v], mm, gl, gr);
             const R Ad = sb[d].v[v] * gl, Bd = sb[d].v[v] * gr;
             own += Ad - Bd;
-            A.QB[(size_t)(9 + 9 * d + v) * I.n + c] = Ad;
-            A.QB[(size_t)(36 + 9 * d + v) * I.n + c] = Bd;
+            A.QB[(size_t)(9 + 9 * d + v) * n + c] = Ad;
+            A.QB[(size_t)(36 + 9 * d + v) * n + c] = Bd;
         }
-        A.QB[(size_t)v * I.n + c] = own;
+        A.QB[(size_t)v * n + c] = own;
     }
+}
+template <class R> GMT_HD void adj_recon_cell(const AdjArgs<R>& A, size_t c) {
+    const Idx<R> I = idx_of(A);
+    int x, y, z;
+    cell_xyz(A, c, x, y, z);
+    CellRec<R> r;
+    cell_rec(A.u, I, x, y, z, A.K, A.dtdx, A.iflo, A.recon == RECON_MINMOD, r);
+    adj_recon_core(A, I.n, c, r, FaceBarGlobal<R>{A.FSb, I.n, c});
 }
 
 // pass 6: gather the primitive adjoint of cell c and map it through cons2prim
