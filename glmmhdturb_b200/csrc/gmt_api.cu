@@ -911,9 +911,13 @@ int gmt_run(gmt_ctx* c, void* u, void* w, int32_t nsteps, double t0, double t_en
 // ------------------------------------------------------------------------------------------
 }  // extern "C"
 
-// z-chunk of an ensemble work item: 32 planes keep the per-chunk prologue (two extra planes) near
-// 6% while a 64-box ensemble still yields thousands of items for the persistent grid
-constexpr int ENS_LZ = 32;
+// z-chunk of a box's ensemble work items: the box's nz split into ceil(n/64) equal chunks, so the
+// per-chunk prologue (two extra planes) stays near 3-6% while a 64-box ensemble still yields
+// thousands of items for the persistent grid
+inline int ens_lz(int n) {
+    const int nch = (n + 63) / 64;
+    return (n + nch - 1) / nch;
+}
 
 struct gmt_ensemble {
     gmt_params p;
@@ -955,7 +959,7 @@ template <class R> int ens_bind(gmt_ensemble* E, void* const* u, void* const* w,
             a.u = cplanes<R>(par == 0 ? u[b] : w[b], cells);
             a.o = planes<R>(par == 0 ? w[b] : u[b], cells);
             a.nx = a.ny = a.nz = n;
-            a.ox = 16; a.oy = 16; a.lz = ENS_LZ;
+            a.ox = ens_tile_x<R>(); a.oy = 16; a.lz = ens_lz(n);
             a.dt = a.dtdx = a.ch = a.glm_fac = a.ramp = R(0);
             a.K = consts_of<R>(E->p);
             a.iflo = E->p.iflo; a.use_llf = E->p.riemann == GMT_RIEMANN_LLF;
@@ -1063,16 +1067,20 @@ int gmt_ensemble_create(const gmt_params* base, int32_t nbox, const int32_t* n, 
         for (int a = 0; a < 3; ++a) A(&E->trig[3 * b + a], (size_t)8 * n[b] * E->esize);
         E->rows_max = std::max(E->rows_max, n[b] * n[b]);
     }
-    // work items: biggest boxes first, 16x16 tiles x ENS_LZ-plane chunks (the last chunk of a box
-    // may be shorter)
+    // work items: biggest boxes first, tiles of ens_tile_x x 16 columns (a box whose width is not a
+    // multiple of the tile gets an overhanging last tile) x ens_lz-plane chunks (the last chunk of
+    // a box may be shorter)
+    const int etx = E->esize == 8 ? ens_tile_x<double>() : ens_tile_x<float>();
     std::vector<int> order(nbox);
     for (int b = 0; b < nbox; ++b) order[b] = b;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
     std::vector<EnsItem> items;
-    for (int b : order)
-        for (int bz = 0; bz < (n[b] + ENS_LZ - 1) / ENS_LZ; ++bz)
+    for (int b : order) {
+        const int lz = ens_lz(n[b]);
+        for (int bz = 0; bz < (n[b] + lz - 1) / lz; ++bz)
             for (int by = 0; by < n[b] / 16; ++by)
-                for (int bx = 0; bx < n[b] / 16; ++bx) items.push_back({b, bx, by, bz});
+                for (int bx = 0; bx < (n[b] + etx - 1) / etx; ++bx) items.push_back({b, bx, by, bz});
+    }
     E->nitems = (int)items.size();
     A((void**)&E->items, items.size() * sizeof(EnsItem));
     if (e == cudaSuccess) e = cudaMemcpy(E->items, items.data(), items.size() * sizeof(EnsItem), cudaMemcpyHostToDevice);

@@ -18,6 +18,8 @@ int unsplit_max_threads(int dtype_bytes);
 cudaError_t unsplit_prepare_f32();   // shared-memory attributes of every step kernel
 cudaError_t unsplit_prepare_f64();
 struct EnsItem;
+// tile of the ensemble kernel: ens_tile_x<R>() columns by 16 rows (32 in FP32, 16 in FP64)
+template <class R> constexpr int ens_tile_x() { return sizeof(R) == 4 ? 32 : 16; }
 cudaError_t launch_ensemble(const UnsplitArgs<float>* boxes, const EnsItem* items, int nitems, unsigned* queue,
                             int recon, int riem, int nsm, cudaStream_t s);
 cudaError_t launch_ensemble(const UnsplitArgs<double>* boxes, const EnsItem* items, int nitems, unsigned* queue,

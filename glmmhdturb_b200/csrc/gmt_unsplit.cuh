@@ -270,7 +270,10 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
 #pragma unroll
     for (int v = 0; v < 9; ++v) { pPz.v[v] = R(0); Fzlo.v[v] = R(0); Fxh.v[v] = R(0); Fyh.v[v] = R(0); }
     double cmax = 0.0, smax = 0.0;
-    const int gx = x0 + tx, gy = y0 + ty;
+    // a tile may overhang the box (an ensemble box narrower than a tile multiple): the overhanging
+    // columns recompute the periodic images of cells at the start of the row, bit for bit the same
+    // values, so their duplicate writes (and CFL maxima) are harmless
+    const int gx = x0 + tx < nx ? x0 + tx : x0 + tx - nx, gy = y0 + ty < ny ? y0 + ty : y0 + ty - ny;
     const int cown = (tx + 2) + PW * (ty + 2);     // ring-local index of the owned cell
     const int rown = (tx + 1) + RW * (ty + 1);     // recon-local index of the owned cell
     const int ixh = (tx + 2) + RW * (ty + 1);      // slot of the +x neighbour

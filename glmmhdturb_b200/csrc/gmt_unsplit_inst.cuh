@@ -92,19 +92,22 @@ template <class R, int MAXT, int MINB> static int unsplit_regs_of_t(int recon, i
 }  // namespace gmt
 
 namespace gmt {
-// ensemble launcher: 16x16 tiles, persistent grid of 2 blocks per SM
+// ensemble launcher: persistent grid, one (FP32) or two (FP64) blocks per SM
 template <class R, int RECON, int RIEM>
 static cudaError_t ensemble_go(const UnsplitArgs<R>* boxes, const EnsItem* items, int nitems, unsigned* queue,
                                int nsm, cudaStream_t s) {
-    auto k = ensemble_kernel<R, RECON, RIEM, 16, 16, 256, 2>;
+    // FP32: 32x16 tiles, 512 threads, one block per SM; FP64: 16x16 tiles, 256 threads
+    constexpr bool F32 = sizeof(R) == 4;
+    constexpr int OX = ens_tile_x<R>(), OY = 16, NT = OX * OY, MB = F32 ? 1 : 2;
+    auto k = ensemble_kernel<R, RECON, RIEM, OX, OY, NT, MB>;
     static int configured[64] = {0};
     {
         cudaError_t e = configure_once(k, configured);
         if (e != cudaSuccess) return e;
     }
     if (nitems <= 0) return cudaSuccess;   // configure only
-    int nb = std::max(1, std::min(nitems, 2 * nsm));
-    k<<<nb, 256, unsplit_smem_bytes<R>(16, 16), s>>>(boxes, items, nitems, queue);
+    int nb = std::max(1, std::min(nitems, MB * nsm));
+    k<<<nb, NT, unsplit_smem_bytes<R>(OX, OY), s>>>(boxes, items, nitems, queue);
     return cudaGetLastError();
 }
 }  // namespace gmt
