@@ -232,7 +232,7 @@ template <class R, int RECON> struct MarchScheme {
 // One tile (bx, by) x z-chunk bz of one box.  TOX, TOY > 0 fix the tile at compile time
 // (constant shared-memory offsets); 0 = runtime tile.  Used by the single-box kernel (one tile per
 // block) and by the ensemble kernel (a queue of tiles over many boxes).
-template <class R, class S, int TOX, int TOY>
+template <class R, class S, int TOX, int TOY, bool OVERHANG = false>
 __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepVals<R>& V, int bx, int by, int bz,
                                             unsigned char* smem_raw) {
     const int OX = TOX > 0 ? TOX : A.ox, OY = TOY > 0 ? TOY : A.oy;
@@ -270,10 +270,14 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
 #pragma unroll
     for (int v = 0; v < 9; ++v) { pPz.v[v] = R(0); Fzlo.v[v] = R(0); Fxh.v[v] = R(0); Fyh.v[v] = R(0); }
     double cmax = 0.0, smax = 0.0;
-    // a tile may overhang the box (an ensemble box narrower than a tile multiple): the overhanging
-    // columns recompute the periodic images of cells at the start of the row, bit for bit the same
-    // values, so their duplicate writes (and CFL maxima) are harmless
-    const int gx = x0 + tx < nx ? x0 + tx : x0 + tx - nx, gy = y0 + ty < ny ? y0 + ty : y0 + ty - ny;
+    // OVERHANG: a tile may overhang the box (an ensemble box narrower than a tile multiple); the
+    // overhanging columns recompute the periodic images of cells at the start of the row, bit for
+    // bit the same values, so their duplicate writes (and CFL maxima) are harmless
+    int gx = x0 + tx, gy = y0 + ty;
+    if (OVERHANG) {
+        gx = gx < nx ? gx : gx - nx;
+        gy = gy < ny ? gy : gy - ny;
+    }
     const int cown = (tx + 2) + PW * (ty + 2);     // ring-local index of the owned cell
     const int rown = (tx + 1) + RW * (ty + 1);     // recon-local index of the owned cell
     const int ixh = (tx + 2) + RW * (ty + 1);      // slot of the +x neighbour
@@ -411,10 +415,10 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     }
 }
 
-template <class R, int RECON, int RIEM, int TOX, int TOY>
+template <class R, int RECON, int RIEM, int TOX, int TOY, bool OVERHANG = false>
 __device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const StepVals<R>& V, int bx, int by, int bz,
                                              unsigned char* smem_raw) {
-    scheme_tile<R, UnsplitScheme<R, RECON, RIEM>, TOX, TOY>(A, V, bx, by, bz, smem_raw);
+    scheme_tile<R, UnsplitScheme<R, RECON, RIEM>, TOX, TOY, OVERHANG>(A, V, bx, by, bz, smem_raw);
 }
 
 // A tile = (box, bx, by, bz) work item of the ensemble kernel.
@@ -436,7 +440,7 @@ __global__ void __launch_bounds__(MAXT, MINB) ensemble_kernel(const UnsplitArgs<
         if (it >= nitems) break;
         const EnsItem w = items[it];
         const UnsplitArgs<R> A = boxes[w.box];
-        unsplit_tile<R, RECON, RIEM, TOX, TOY>(A, step_vals(A), w.bx, w.by, w.bz, smem_raw);
+        unsplit_tile<R, RECON, RIEM, TOX, TOY, true>(A, step_vals(A), w.bx, w.by, w.bz, smem_raw);
         __syncthreads();
     }
 }
