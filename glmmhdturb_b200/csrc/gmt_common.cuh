@@ -1,5 +1,6 @@
 // gmt_common.cuh -- kernel argument blocks and small device helpers shared by the kernels.
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -130,9 +131,22 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long* d
 template <class R>
 __device__ __forceinline__ void cfl_speeds(const Q9<R>& c, const Consts<R>& K, R& ctot, R& smax) {
     Q9<R> q = cons2prim(c, K.gamma, K.smallr, K.pfl);
-    R sx = rabs(q.v[1]) + fast_speed(q, K.gamma, q.v[5]);
-    R sy = rabs(q.v[2]) + fast_speed(q, K.gamma, q.v[6]);
-    R sz = rabs(q.v[3]) + fast_speed(q, K.gamma, q.v[7]);
+    R sx, sy, sz;
+    if constexpr (std::is_same<R, float>::value) {
+        // FP32: the three fast speeds share 1/rho, c^2 and d^2 (fast_speed's expressions with the
+        // division by rho taken once, as the fast-math build evaluates it anyway)
+        const R ir = R(1) / q.v[0];
+        const R c2 = K.gamma * q.v[4] * ir;
+        const R b2 = (q.v[5] * q.v[5] + q.v[6] * q.v[6] + q.v[7] * q.v[7]) * ir;
+        const R d2 = R(0.5) * (b2 + c2), t = c2 * ir;
+        sx = rabs(q.v[1]) + rsqrt_ieee(d2 + rsqrt_ieee(rmax(d2 * d2 - t * q.v[5] * q.v[5], R(0))));
+        sy = rabs(q.v[2]) + rsqrt_ieee(d2 + rsqrt_ieee(rmax(d2 * d2 - t * q.v[6] * q.v[6], R(0))));
+        sz = rabs(q.v[3]) + rsqrt_ieee(d2 + rsqrt_ieee(rmax(d2 * d2 - t * q.v[7] * q.v[7], R(0))));
+    } else {
+        sx = rabs(q.v[1]) + fast_speed(q, K.gamma, q.v[5]);
+        sy = rabs(q.v[2]) + fast_speed(q, K.gamma, q.v[6]);
+        sz = rabs(q.v[3]) + fast_speed(q, K.gamma, q.v[7]);
+    }
     ctot = sx + sy + sz;
     smax = rmax(rmax(sx, sy), sz);
 }

@@ -269,7 +269,7 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     Q9<R> pPz, Fzlo, Fxh, Fyh;
 #pragma unroll
     for (int v = 0; v < 9; ++v) { pPz.v[v] = R(0); Fzlo.v[v] = R(0); Fxh.v[v] = R(0); Fyh.v[v] = R(0); }
-    double cmax = 0.0, smax = 0.0;
+    R cmax = R(0), smax = R(0);   // exact maxima in R, widened to FP64 once per block
     // OVERHANG: a tile may overhang the box (an ensemble box narrower than a tile multiple); the
     // overhanging columns recompute the periodic images of cells at the start of the row, bit for
     // bit the same values, so their duplicate writes (and CFL maxima) are harmless
@@ -343,8 +343,8 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
                     if (A.cfl_out) {
                         R ct, sg;
                         cfl_speeds(q, K, ct, sg);
-                        cmax = fmax(cmax, (double)ct);
-                        smax = fmax(smax, (double)sg);
+                        cmax = fmax(cmax, ct);
+                        smax = fmax(smax, sg);
                     }
                 }
                 Fzlo = Fzhi;
@@ -409,9 +409,9 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     }
     if (tid == 0) mbar_inval(mbar);
     if (A.cfl_out) {
-        block_max_atomic(cmax, A.cfl_out, red);
+        block_max_atomic((double)cmax, A.cfl_out, red);
         __syncthreads();
-        block_max_atomic(smax, A.cfl_out + 1, red);
+        block_max_atomic((double)smax, A.cfl_out + 1, red);
     }
 }
 
