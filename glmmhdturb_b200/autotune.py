@@ -20,7 +20,7 @@ TILES = {
     "f32": [(32, 8), (16, 8), (16, 16), (32, 4), (64, 4), (32, 16), (64, 8), (16, 32), (128, 4)],
     "f64": [(32, 8), (16, 8), (16, 16), (32, 4), (8, 8)],
 }
-CHUNKS = [16, 32, 64, 128, 0]
+CHUNKS = [16, 32, 64, 128, 256, 0]
 
 
 def _key(n, dtype, scheme, recon, riemann):
