@@ -252,6 +252,13 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     const R dtdx = V.dtdx, ch = V.ch;
     const bool turb = A.do_turb && A.btab != nullptr;
     const int nhelp = 2 * (OX + OY);
+    // The extra work of a plane is packed into whole warps: halo reconstructions on the first
+    // warps (phase R), boundary faces on the last ones (phase F).  The plane's staging copies skip
+    // the helper warps and its primitive conversion skips the boundary-face warps, so both
+    // phases' barrier tails shrink by that share (when at least one other warp remains).
+    const int hwarp = 32 * ((nhelp + 31) / 32), bwarp = 32 * ((OX + OY + 31) / 32);
+    const int stg0 = NT - hwarp >= 32 ? hwarp : 0;                 // first staging thread
+    const int nunst = NT - bwarp >= 32 ? NT - bwarp : NT;          // unstaging threads [0, nunst)
 
     // prologue: primitives of planes z0-2, z0-1, z0
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
@@ -293,7 +300,7 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
         const bool load = kr + 2 <= z1 + 1;
         const int s0 = mod3(kr), sm = mod3(kr - 1), sp = mod3(kr + 1);
         if (load) {
-            stage_plane(SG, A.u, PN, PW, x0, y0, kr + 2, nx, ny, nz, tid, NT);
+            stage_plane(SG, A.u, PN, PW, x0, y0, kr + 2, nx, ny, nz, tid >= stg0 ? tid - stg0 : PN, NT - stg0);
             mbar_arrive_cp_async(mbar);
         }
         {
@@ -403,7 +410,7 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
         if (load) {
             mbar_wait(mbar, phase, A.err);
             phase ^= 1u;
-            unstage_plane(PR + mod3(kr + 2) * 9 * PN, SG, PN, K, S::prim_floor(K), tid, NT);
+            unstage_plane(PR + mod3(kr + 2) * 9 * PN, SG, PN, K, S::prim_floor(K), tid < nunst ? tid : PN, nunst);
         }
         __syncthreads();
     }

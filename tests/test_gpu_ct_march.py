@@ -212,3 +212,60 @@ def test_ct_turbulent_state_is_divergence_free(dtype):
         s.step(q, w, 0.3 * s.dx / cm, ch=1.0, glm_fac=1.0)
         q, w = w, q
     assert s.ct_divb_max(q) <= 10 * tol and bool(torch.isfinite(q).all())
+
+
+@pytest.mark.parametrize("scheme,recon,riem", [("unsplit", "mc", "hlld"), ("unsplit", "ppm", "hll"),
+                                               ("march1d", "mc", "hll"), ("ct", "mc", "hlld"), ("ct", "ppm", "hll")])
+def test_fp32_production_tile_vs_oracle(oracle, scheme, recon, riem):
+    """The FP32 step kernels specialised at compile time for the 32x16 production tile (the shape
+    the autotuner picks at 512^3) against the FP64 oracle on a 64x32x16 grid, three steps, and
+    against the same FP32 step on a runtime 16x16 tile."""
+    import math
+    from glmmhdturb_b200 import Solver
+    from tests.gpu_util import perturbed_glm_state
+    n = (64, 32, 16)
+    if scheme == "ct":
+        cfg = oracle.Config(n=n, gamma=5 / 3, recon=recon, riemann=riem, emf="contact")
+        u0 = oracle.ct_ic_ot(cfg)
+        rng = np.random.default_rng(5)
+        u0[1:4] += 0.05 * rng.standard_normal(u0[1:4].shape)
+    else:
+        cfg = oracle.Config(n=n, gamma=5 / 3, recon=recon, riemann=riem)
+        u0 = perturbed_glm_state(oracle, n, seed=11, gamma=5 / 3)
+    kw = dict(dtype="f32", scheme=scheme, recon=recon, riemann=riem, gamma=5 / 3)
+    if scheme == "ct":
+        kw["emf"] = "contact"
+    if scheme == "march1d":
+        kw["smallp"] = cfg.smallp
+    outs = {}
+    for tile in ((32, 16, 0), (16, 16, 0)):
+        s = Solver(n, tile=tile, **kw)
+        assert s.kernel_info()["tile"][:2] == tile[:2]
+        q = to_dev(u0, torch.float32)
+        w = torch.empty_like(q)
+        ref = u0
+        for _ in range(3):
+            if scheme == "ct":
+                cmax, _ = oracle.ct_cfl(cfg, ref)
+                dt = 0.3 * cfg.dx / cmax
+                ref = oracle.ct_step(cfg, ref, dt)
+                s.step(q, w, dt)
+            else:
+                cmax, smax = oracle.cfl(cfg, ref)
+                dt = 0.3 * cfg.dx / cmax
+                fac = math.exp(-(smax / 0.18) * dt)
+                if scheme == "march1d":
+                    ref = oracle.step_march1d(cfg, ref, dt, smax, fac)
+                else:
+                    ref = oracle.step_unsplit(cfg, ref, dt, smax, fac)
+                s.step(q, w, dt, ch=smax, glm_fac=fac)
+            q, w = w, q
+        got = q.cpu().numpy()
+        err, errs = max_rel_err(got, ref)
+        # the 8 MHD fields to FP32 round-off; the GLM psi is a small field sourced by round-off
+        assert max(errs[:8]) <= 3e-5, (tile, errs)
+        if scheme != "ct":
+            assert errs[8] <= 1e-2, (tile, errs)
+        outs[tile] = got
+    err, errs = max_rel_err(outs[(32, 16, 0)], outs[(16, 16, 0)].astype(np.float64))
+    assert max(errs[:8]) <= 1e-5, errs
