@@ -176,6 +176,11 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
     const R dtdx = A.dtdx;
     const bool turb = A.do_turb && A.btab != nullptr;
     const int nhelp = 2 * (OX + OY);
+    // staging skips the helper warps, the primitive conversion the boundary-face warps (the two
+    // phases' barrier tails; as in the GLM tile march)
+    const int hwarp = 32 * ((nhelp + 31) / 32), bwarp = 32 * ((OX + OY + 31) / 32);
+    const int stg0 = NT - hwarp >= 32 ? hwarp : 0;
+    const int nunst = NT - bwarp >= 32 ? NT - bwarp : NT;
     R* S = A.scratch;
 
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
@@ -205,7 +210,7 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
         const int s0 = mod3(kr), sm = mod3(kr - 1), sp = mod3(kr + 1);
         const R* FB0 = FB + (size_t)s0 * 3 * PN;
         if (load) {
-            ct_stage_plane(SG, A.q, PN5, PW5, x0, y0, kr + 2, nx, ny, nz, tid, NT);
+            ct_stage_plane(SG, A.q, PN5, PW5, x0, y0, kr + 2, nx, ny, nz, tid >= stg0 ? tid - stg0 : PN5, NT - stg0);
             mbar_arrive_cp_async(mbar);
         }
         {
@@ -321,7 +326,8 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
         if (load) {
             mbar_wait(mbar, phase, A.err);
             phase ^= 1u;
-            ct_unstage_plane(PR + mod3(kr + 2) * 9 * PN, FB + mod3(kr + 2) * 3 * PN, SG, PN, PW, PN5, PW5, K, tid, NT);
+            ct_unstage_plane(PR + mod3(kr + 2) * 9 * PN, FB + mod3(kr + 2) * 3 * PN, SG, PN, PW, PN5, PW5, K,
+                             tid < nunst ? tid : PN, nunst);
         }
         __syncthreads();
     }
