@@ -282,11 +282,8 @@ template <int RIEM, class R> GMT_HD void adj_flux_cell(const AdjArgs<R>& A, size
 
 // pass 3: the update and its epilogue; returns this cell's part of dL/d(amplitude)
 template <class R> GMT_HD double adj_update_cell(const AdjArgs<R>& A, size_t c) {
-    constexpr int NU = 6;
-    using DD = Dual<R, NU>;
     const Idx<R> I = idx_of(A);
     const bool turb = A.do_turb && A.btab != nullptr;
-    const Consts<DD> KD = dual_consts<R, NU>(A.K);
     int x, y, z;
     cell_xyz(A, c, x, y, z);
     const size_t cxm = I.at(x - 1, y, z), cym = I.at(x, y - 1, z), czm = I.at(x, y, z - 1);
@@ -302,7 +299,26 @@ template <class R> GMT_HD double adj_update_cell(const AdjArgs<R>& A, size_t c) 
     if (turb) force_accel(A.btab + ((size_t)z * A.ny + y) * 24, A.trigx, A.nx, x, A.ramp, a3[0], a3[1], a3[2]);
     const Q9<R> ob = load_u(A.ubn, c);
     Q9<R> rb;
-    R abar[3] = {R(0), R(0), R(0)};
+    R abar[3];
+    finish_update_adj(r1, A.K, A.glm_fac, turb, a3[0], a3[1], a3[2], A.dt, ob, rb, abar);
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+        A.R1b[(size_t)v * I.n + c] = rb.v[v];
+        A.ub.p[v][c] = rb.v[v];
+    }
+    if (turb && A.amp != R(0))
+        return ((double)abar[0] * a3[0] + (double)abar[1] * a3[1] + (double)abar[2] * a3[2]) / (double)A.amp;
+    return 0.0;
+}
+
+// the same epilogue adjoint by forward-mode dual numbers over the 12 inputs (9 state, 3
+// accelerations); the reference the hand-written sweep is checked against
+template <class R>
+GMT_HD void finish_update_adj_dual(const Q9<R>& r1, const Consts<R>& K, R glm_fac, bool turb, const R a3[3], R dt,
+                                   const Q9<R>& ob, Q9<R>& rb, R abar[3]) {
+    constexpr int NU = 6;
+    using DD = Dual<R, NU>;
+    const Consts<DD> KD = dual_consts<R, NU>(K);
 #pragma unroll
     for (int c0 = 0; c0 < 12; c0 += NU) {   // two passes: the 9 state inputs, then the 3 accelerations
         Q9<DD> q;
@@ -319,7 +335,7 @@ template <class R> GMT_HD double adj_update_cell(const AdjArgs<R>& A, size_t c) 
 #pragma unroll
             for (int j = 0; j < NU; ++j) ad[i].d[j] = (c0 + j == 9 + i) ? R(1) : R(0);
         }
-        finish_update(q, KD, DD(A.glm_fac), turb, ad[0], ad[1], ad[2], DD(A.dt));
+        finish_update(q, KD, DD(glm_fac), turb, ad[0], ad[1], ad[2], DD(dt));
 #pragma unroll
         for (int j = 0; j < NU; ++j) {
             R acc = R(0);
@@ -330,14 +346,6 @@ template <class R> GMT_HD double adj_update_cell(const AdjArgs<R>& A, size_t c) 
             else if (i < 12) abar[i - 9] = acc;
         }
     }
-#pragma unroll
-    for (int v = 0; v < 9; ++v) {
-        A.R1b[(size_t)v * I.n + c] = rb.v[v];
-        A.ub.p[v][c] = rb.v[v];
-    }
-    if (turb && A.amp != R(0))
-        return ((double)abar[0] * a3[0] + (double)abar[1] * a3[1] + (double)abar[2] * a3[2]) / (double)A.amp;
-    return 0.0;
 }
 
 // pass 4: adjoint of the Riemann solves at the +x, +y, +z faces of cell c

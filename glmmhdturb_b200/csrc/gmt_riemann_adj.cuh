@@ -547,4 +547,86 @@ GMT_HD bool riemann_x_adj(const Q9<R>& Lq, const Q9<R>& Rq, const Q9<R>& fb, con
     return true;
 }
 
+
+// Reverse sweep of the update epilogue finish_update (void floor, psi damping, forcing kick;
+// glmmhd_turb.jl:450-475): given the output adjoint ob, the adjoint rb of the pre-epilogue state
+// r and ab of the three accelerations.  A max(a, b) passes its adjoint to a when a >= b, as the
+// dual-number evaluation of the forward does.
+template <class R>
+GMT_HD void finish_update_adj(const Q9<R>& rin, const Consts<R>& K, R glm_fac, bool turb, R ax, R ay, R az, R dt,
+                              const Q9<R>& ob, Q9<R>& rb, R ab[3]) {
+    Q9<R> r = rin;
+    const bool voidf = r.v[0] < K.smallr;
+    if (voidf) {
+        r.v[0] = K.smallr; r.v[1] = R(0); r.v[2] = R(0); r.v[3] = R(0);
+        r.v[4] = K.pfl / (K.gamma - R(1)) + R(0.5) * (r.v[5] * r.v[5] + r.v[6] * r.v[6] + r.v[7] * r.v[7]);
+    }
+    Q9<R> b = ob;   // adjoint of the state after the void floor (psi handled below)
+    ab[0] = ab[1] = ab[2] = R(0);
+    if (turb && r.v[0] >= K.turb_min_rho) {
+        const R rho = r.v[0], rhom = rmax(rho, K.smallr), irm = R(1) / rhom;
+        const R fl = rho * (K.smallc * K.smallc);
+        const R acc[3] = {ax, ay, az};
+        // forward values and branch flags of the six floored energy updates
+        R e = r.v[4], m[3];
+        bool t[6];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const R x = e - R(0.5) * r.v[1 + i] * r.v[1 + i] / rhom;
+            t[i] = x >= fl;
+            e = t[i] ? x : fl;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) m[i] = r.v[1 + i] + rhom * acc[i] * dt;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const R x = e + R(0.5) * m[i] * m[i] / rhom;
+            t[3 + i] = x >= fl;
+            e = t[3 + i] ? x : fl;
+        }
+        // reverse
+        R eb = ob.v[4], flb = R(0), rhomb = R(0);
+        R mb[3] = {ob.v[1], ob.v[2], ob.v[3]};
+        R vb[3] = {R(0), R(0), R(0)};
+#pragma unroll
+        for (int i = 2; i >= 0; --i) {
+            if (t[3 + i]) {
+                mb[i] += eb * m[i] * irm;
+                rhomb -= eb * R(0.5) * m[i] * m[i] * irm * irm;
+            } else {
+                flb += eb;
+                eb = R(0);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            vb[i] += mb[i];
+            rhomb += mb[i] * acc[i] * dt;
+            ab[i] = mb[i] * rhom * dt;
+        }
+#pragma unroll
+        for (int i = 2; i >= 0; --i) {
+            if (t[i]) {
+                vb[i] -= eb * r.v[1 + i] * irm;
+                rhomb += eb * R(0.5) * r.v[1 + i] * r.v[1 + i] * irm * irm;
+            } else {
+                flb += eb;
+                eb = R(0);
+            }
+        }
+        b.v[1] = vb[0]; b.v[2] = vb[1]; b.v[3] = vb[2];
+        b.v[4] = eb;
+        b.v[0] = ob.v[0] + flb * (K.smallc * K.smallc) + (rho >= K.smallr ? rhomb : R(0));
+    }
+    rb = b;
+    rb.v[8] = ob.v[8] * glm_fac;
+    if (voidf) {
+        // rho, momentum and E were overwritten: only B reaches E through the magnetic energy
+        rb.v[5] += b.v[4] * r.v[5];
+        rb.v[6] += b.v[4] * r.v[6];
+        rb.v[7] += b.v[4] * r.v[7];
+        rb.v[0] = rb.v[1] = rb.v[2] = rb.v[3] = rb.v[4] = R(0);
+    }
+}
+
 }  // namespace gmt
