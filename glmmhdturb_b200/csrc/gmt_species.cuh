@@ -42,19 +42,32 @@ template <class R>
 __global__ void __launch_bounds__(128) species_kernel(const MarchArgs<R> A, const R* __restrict__ fmass) {
     const size_t n = (size_t)A.nx * A.ny * A.nz;
     const R h = R(0.5) * A.dtdx;
+    const size_t sxy = (size_t)A.nx * A.ny;
     for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(g % A.nx), y = (int)((g / A.nx) % A.ny), z = (int)(g / ((size_t)A.nx * A.ny));
+        int x, y, z;
+        if (n <= 0xffffffffu) {   // 32-bit divisions for every linear index below 2^32
+            const unsigned gg = (unsigned)g, q = gg / (unsigned)A.nx;
+            x = (int)(gg - q * (unsigned)A.nx);
+            y = (int)(q % (unsigned)A.ny);
+            z = (int)(q / (unsigned)A.ny);
+        } else {
+            x = (int)(g % A.nx); y = (int)((g / A.nx) % A.ny); z = (int)(g / sxy);
+        }
         R divs[MAX_SPECIES];
 #pragma unroll
         for (int s = 0; s < MAX_SPECIES; ++s) divs[s] = R(0);
 #pragma unroll
         for (int D = 0; D < 3; ++D) {
+            // the stencil g + (i - c) * stride along D, i the periodic image of c + k - 2
+            const int c = D == 0 ? x : (D == 1 ? y : z), m = D == 0 ? A.nx : (D == 1 ? A.ny : A.nz);
+            const size_t st = D == 0 ? 1 : (D == 1 ? (size_t)A.nx : sxy);
             size_t at[5];
 #pragma unroll
             for (int k = 0; k < 5; ++k) {
-                const int sft = k - 2;
-                const int xx = x + (D == 0 ? sft : 0), yy = y + (D == 1 ? sft : 0), zz = z + (D == 2 ? sft : 0);
-                at[k] = (size_t)wrapi(xx, A.nx) + (size_t)A.nx * ((size_t)wrapi(yy, A.ny) + (size_t)A.ny * wrapi(zz, A.nz));
+                int i = c + k - 2;
+                i = i < 0 ? i + m : (i >= m ? i - m : i);
+                i = i < 0 ? i + m : (i >= m ? i - m : i);   // boxes narrower than the stencil
+                at[k] = g + (size_t)((long long)(i - c) * (long long)st);
             }
             R rho[5], un[3];
 #pragma unroll
