@@ -108,6 +108,22 @@ template <class R> __device__ __forceinline__ void cp_async_r(R* smem, const R* 
 template <> __device__ __forceinline__ void cp_async_r(float* s, const float* g) { cp_async4(s, g); }
 template <> __device__ __forceinline__ void cp_async_r(double* s, const double* g) { cp_async8(s, g); }
 
+// coordinates of linear cell index c = x + nx (y + ny z); 32-bit divisions while n < 2^32
+GMT_HD void cell_coords(size_t c, int nx, int ny, size_t n, int& x, int& y, int& z) {
+    if (n <= 0xffffffffu) {
+        const unsigned cc = (unsigned)c, q = cc / (unsigned)nx;
+        x = (int)(cc - q * (unsigned)nx);
+        y = (int)(q % (unsigned)ny);
+        z = (int)(q / (unsigned)ny);
+    } else {
+        x = (int)(c % nx);
+        y = (int)((c / nx) % ny);
+        z = (int)(c / ((size_t)nx * ny));
+    }
+}
+// periodic image of i for -n <= i < 2n
+GMT_HD int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
 GMT_HD int wrapi(int i, int n) {
     i = i % n;
     return i < 0 ? i + n : i;

@@ -354,10 +354,11 @@ template <class R> __global__ void __launch_bounds__(256) ct_edge_kernel(const C
     R* W = A.scratch;
     const bool contact = A.emf == 1;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((size_t)nx * ny));
-        const size_t xm = (size_t)wrapi(x - 1, nx) + (size_t)nx * (y + (size_t)ny * z);
-        const size_t ym = (size_t)x + (size_t)nx * (wrapi(y - 1, ny) + (size_t)ny * z);
-        const size_t zm = (size_t)x + (size_t)nx * (y + (size_t)ny * wrapi(z - 1, nz));
+        int x, y, z;
+        cell_coords(c, nx, ny, n, x, y, z);
+        const size_t xm = (size_t)wrap1(x - 1, nx) + (size_t)nx * (y + (size_t)ny * z);
+        const size_t ym = (size_t)x + (size_t)nx * (wrap1(y - 1, ny) + (size_t)ny * z);
+        const size_t zm = (size_t)x + (size_t)nx * (y + (size_t)ny * wrap1(z - 1, nz));
 #pragma unroll
         for (int e = 0; e < 3; ++e) {
             // A = (e+1)%3, B = (e+2)%3; c10 = one step back along A, c01 along B, c11 along both
@@ -365,15 +366,15 @@ template <class R> __global__ void __launch_bounds__(256) ct_edge_kernel(const C
             int ea, eb, ma, mb, ec;
             if (e == 2) {        // (A,B) = (x,y)
                 c10 = xm; c01 = ym;
-                c11 = (size_t)wrapi(x - 1, nx) + (size_t)nx * (wrapi(y - 1, ny) + (size_t)ny * z);
+                c11 = (size_t)wrap1(x - 1, nx) + (size_t)nx * (wrap1(y - 1, ny) + (size_t)ny * z);
                 ea = CS_EZX; eb = CS_EZY; ma = CS_MX; mb = CS_MY; ec = CS_ECZ;
             } else if (e == 0) { // (A,B) = (y,z)
                 c10 = ym; c01 = zm;
-                c11 = (size_t)x + (size_t)nx * (wrapi(y - 1, ny) + (size_t)ny * wrapi(z - 1, nz));
+                c11 = (size_t)x + (size_t)nx * (wrap1(y - 1, ny) + (size_t)ny * wrap1(z - 1, nz));
                 ea = CS_EXY; eb = CS_EXZ; ma = CS_MY; mb = CS_MZ; ec = CS_ECX;
             } else {             // (A,B) = (z,x)
                 c10 = zm; c01 = xm;
-                c11 = (size_t)wrapi(x - 1, nx) + (size_t)nx * (y + (size_t)ny * wrapi(z - 1, nz));
+                c11 = (size_t)wrap1(x - 1, nx) + (size_t)nx * (y + (size_t)ny * wrap1(z - 1, nz));
                 ea = CS_EYZ; eb = CS_EYX; ma = CS_MZ; mb = CS_MX; ec = CS_ECY;
             }
             const R EaN = S[ea * n + c], EaS = S[ea * n + c01];
@@ -401,10 +402,11 @@ template <class R> __global__ void __launch_bounds__(256) ct_face_kernel(const C
     const R* ez = A.scratch + CS_EDZ * n;
     const R dtdx = A.dtdx;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((size_t)nx * ny));
-        const size_t cxp = (size_t)wrapi(x + 1, nx) + (size_t)nx * (y + (size_t)ny * z);
-        const size_t cyp = (size_t)x + (size_t)nx * (wrapi(y + 1, ny) + (size_t)ny * z);
-        const size_t czp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrapi(z + 1, nz));
+        int x, y, z;
+        cell_coords(c, nx, ny, n, x, y, z);
+        const size_t cxp = (size_t)wrap1(x + 1, nx) + (size_t)nx * (y + (size_t)ny * z);
+        const size_t cyp = (size_t)x + (size_t)nx * (wrap1(y + 1, ny) + (size_t)ny * z);
+        const size_t czp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrap1(z + 1, nz));
         A.o.p[5][c] = A.q.p[5][c] - dtdx * ((ez[cyp] - ez[c]) - (ey[czp] - ey[c]));
         A.o.p[6][c] = A.q.p[6][c] - dtdx * ((ex[czp] - ex[c]) - (ez[cxp] - ez[c]));
         A.o.p[7][c] = A.q.p[7][c] - dtdx * ((ey[cxp] - ey[c]) - (ex[cyp] - ex[c]));
