@@ -264,8 +264,8 @@ class Solver:
 
 class Ensemble:
     """Many periodic GLM boxes of different sizes advanced together: one persistent kernel per step
-    over a queue of 16x16x16 tiles of all boxes, every box with its own dt, forcing amplitude and
-    seed (gmt_ensemble_*)."""
+    over a queue of tile work items of all boxes (32x16 columns in FP32, 16x16 in FP64, z-chunks of
+    at most 64 planes), every box with its own dt, forcing amplitude and seed (gmt_ensemble_*)."""
 
     def __init__(self, sizes, *, amps=None, seeds=None, dtype="f32", recon="mc", riemann="hlld", gamma=5.0 / 3.0,
                  courant=0.3, turb_T=0.5, turb_ndt=100, **kw):

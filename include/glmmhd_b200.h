@@ -139,7 +139,8 @@ int gmt_run(gmt_ctx* ctx, void* u, void* w, int32_t nsteps, double t0, double t_
 /* --- batched ensemble: many periodic boxes of different sizes in one persistent launch per step -
  * (no counterpart in the reference).  Every box: its own n^3 grid (n a multiple of 16), forcing
  * amplitude and seed; the physics of `base`.  Each step: one tick per box, the conditional forcing
- * updates, and one persistent kernel over a queue of 16x16x16 work items of all boxes. */
+ * updates, and one persistent kernel over a queue of tile work items of all boxes (32x16 columns
+ * in FP32, 16x16 in FP64, z-chunks of at most 64 planes). */
 typedef struct gmt_ensemble gmt_ensemble;
 int gmt_ensemble_create(const gmt_params* base, int32_t nbox, const int32_t* n, const double* turb_amp,
                         const uint32_t* seeds, gmt_ensemble** out);
