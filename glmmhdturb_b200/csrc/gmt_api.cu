@@ -93,6 +93,9 @@ struct gmt_ctx {
     double sigma0 = 0, alpha = 0, beta = 0;
     void* adj = nullptr;           // adjoint scratch (207 planes, allocated on first use)
     double* adj_damp = nullptr;    // dL/d(turb_amp) accumulator
+    struct TmaMap { const void* base; CUtensorMap map; };
+    TmaMap tma[2] = {};            // tensor maps of the last two input states (FP32 tile staging)
+    int tma_next = 0;
 };
 
 namespace {
@@ -142,6 +145,64 @@ int choose_tile(gmt_ctx* c, bool ct = false) {
     return GMT_OK;
 }
 
+// cuTensorMapEncodeTiled, looked up once through the runtime (the library does not link libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// The FP32 tile march stages its planes by TMA when the input state is one array of 9 planes
+// (plane stride nx*ny*nz), 16-byte aligned, with nx and the tile width multiples of 4 (16-byte
+// rows and box origins): a 4-D map (x, y, z, variable) whose box is the tile's staged region,
+// (ox+8) x (oy+4) x 1 plane x 9 variables.  Otherwise use_tma stays 0 and every tile uses cp.async.
+template <class R> void set_tma(gmt_ctx* c, UnsplitArgs<R>& A) {
+    A.use_tma = 0;
+    std::memset(&A.tmap, 0, sizeof(A.tmap));
+    if (sizeof(R) != 4) return;
+    const int nx = A.nx, ny = A.ny, nz = A.nz, ox = A.ox, oy = A.oy;
+    if (nx % 4 != 0 || ox % 4 != 0 || ox + 8 > 256 || oy + 4 > 256 || nx < ox + 8 || ny < oy + 4) return;
+    const size_t n = (size_t)nx * ny * nz;
+    const R* base = A.u.p[0];
+    for (int v = 1; v < 9; ++v)
+        if (A.u.p[v] != base + (size_t)v * n) return;
+    if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return;
+    for (const gmt_ctx::TmaMap& t : c->tma)
+        if (t.base == base) {
+            A.tmap = t.map;
+            A.use_tma = 1;
+            return;
+        }
+    EncodeTiledFn enc = encode_tiled_fn();
+    if (!enc) return;
+    CUtensorMap m;
+    const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, 9};
+    const cuuint64_t strides[3] = {(cuuint64_t)nx * sizeof(R), (cuuint64_t)nx * ny * sizeof(R), (cuuint64_t)n * sizeof(R)};
+    const cuuint32_t box[4] = {(cuuint32_t)(ox + 8), (cuuint32_t)(oy + 4), 1, 9};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<R*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return;
+    c->tma[c->tma_next].base = base;
+    c->tma[c->tma_next].map = m;
+    c->tma_next ^= 1;
+    A.tmap = m;
+    A.use_tma = 1;
+}
+
 template <class R> CPlanes<R> cplanes(const void* base, size_t n) {
     CPlanes<R> P;
     for (int v = 0; v < 9; ++v) P.p[v] = static_cast<const R*>(base) + (size_t)v * n;
@@ -177,6 +238,7 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.dx = (R)dx;
         A.dparams = nullptr;
         A.fmass = nullptr;
+        set_tma(c, A);
         if (a->want_cfl) {
             GMT_CUDA(cudaMemsetAsync(c->cfl, 0, 2 * sizeof(unsigned long long), s));
             A.cfl_out = c->cfl;
@@ -206,6 +268,7 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.dx = (R)dx;
         A.dparams = nullptr;
         A.fmass = p.nsp > 0 ? static_cast<R*>(c->fmass) : nullptr;
+        set_tma(c, A);
         if (a->want_cfl) {
             GMT_CUDA(cudaMemsetAsync(c->cfl, 0, 2 * sizeof(unsigned long long), s));
             A.cfl_out = c->cfl;
@@ -832,6 +895,7 @@ cudaError_t run_enqueue(gmt_ctx* c, const void* src, void* dst, int flags, cudaS
     A.dx = (R)(p.boxlen / p.nx);
     A.dparams = reinterpret_cast<const double*>(c->loop);
     A.fmass = nullptr;
+    set_tma(c, A);
     int riem = p.riemann == GMT_RIEMANN_LLF ? GMT_RIEMANN_HLLD : p.riemann;
     return launch_unsplit(A, p.recon, riem, s);
 }
@@ -971,6 +1035,8 @@ template <class R> int ens_bind(gmt_ensemble* E, void* const* u, void* const* w,
             a.dx = (R)(E->p.boxlen / n);
             a.dparams = reinterpret_cast<const double*>(E->loop + b);
             a.fmass = nullptr;
+            a.use_tma = 0;   // the ensemble kernel stages by cp.async
+            std::memset(&a.tmap, 0, sizeof(a.tmap));
         }
     cudaError_t e = cudaMemcpy(E->args, A.data(), A.size() * sizeof(UnsplitArgs<R>), cudaMemcpyHostToDevice);
     return e == cudaSuccess ? GMT_OK : cuda_fail(e, "ensemble bind");

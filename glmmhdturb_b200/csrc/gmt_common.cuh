@@ -1,6 +1,7 @@
 // gmt_common.cuh -- kernel argument blocks and small device helpers shared by the kernels.
 #pragma once
 #include <type_traits>
+#include <cuda.h>   // CUtensorMap (the type only; the library does not link libcuda)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -36,6 +37,8 @@ template <class R> struct UnsplitArgs {
     const double* dparams; // if set: dt, ch, glm_fac, ramp of this step read from device memory
     R* fmass;              // if set: the mass fluxes of every cell's lower x, y, z faces (3 planes),
                            // for the passive-species pass of the march scheme
+    int use_tma;           // tmap describes u: tiles clear of the box edges stage by TMA
+    CUtensorMap tmap;      // 4-D map (x, y, z, variable) of u; box (ox+8) x (oy+4) x 1 x 9
 };
 
 // step values of one box, from the kernel arguments or from device memory
@@ -96,6 +99,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
+// TMA (cp.async.bulk.tensor) staging: one elected thread arms the mbarrier with the byte count of
+// the box and issues the copy; the mbarrier phase completes when the bytes have landed.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(s), "r"(bytes) : "memory");
+}
+// make an initialised mbarrier visible to the async (TMA) proxy
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// order this CTA's earlier generic-proxy accesses of shared memory before later async-proxy ones
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// 4-D tiled load of the box at (c0, c1, c2, c3) into shared memory; the map must live in
+// kernel-parameter (grid-constant), constant or global memory
+__device__ __forceinline__ void tma_load_4d(void* smem_dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(d),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(b)
+        : "memory");
+}
+
 // bounded wait: gives up after ~2^20 polls, records the failure and returns false
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err) {
     for (int it = 0; it < (1 << 20); ++it)

@@ -98,36 +98,50 @@ __device__ __forceinline__ int mod3(int k) {
     return m < 0 ? m + 3 : m;
 }
 
+// The staging plane SG holds the conserved variables of the ring region (x0-2.., y0-2..) with a
+// row pitch SW = OX + 8 and the region starting at column 2: exactly the box (x0-4, y0-2) of
+// (OX+8) x (OY+4) cells that one TMA copy delivers (its first column 16-byte aligned).
 template <class R>
-__device__ __forceinline__ void stage_plane(R* __restrict__ SG, const CPlanes<R>& u, int PN, int PW, int x0, int y0,
-                                            int kp, int nx, int ny, int nz, int tid, int nt) {
+__device__ __forceinline__ void stage_plane(R* __restrict__ SG, const CPlanes<R>& u, int PN, int PW, int SW, int SN,
+                                            int x0, int y0, int kp, int nx, int ny, int nz, int tid, int nt) {
     const int gz = wrapi(kp, nz);
     for (int c = tid; c < PN; c += nt) {
         int lx = c % PW, ly = c / PW;
         int gx = wrapi(x0 - 2 + lx, nx), gy = wrapi(y0 - 2 + ly, ny);
         size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * gz);
+        const int cs = ly * SW + lx + 2;
 #pragma unroll
-        for (int v = 0; v < 9; ++v) cp_async_r(SG + v * PN + c, u.p[v] + g);
+        for (int v = 0; v < 9; ++v) cp_async_r(SG + v * SN + cs, u.p[v] + g);
     }
     cp_async_commit();
 }
 
 template <class R>
-__device__ __forceinline__ void unstage_plane(R* __restrict__ PRs, const R* __restrict__ SG, int PN, const Consts<R>& K,
-                                              R pfloor, int tid, int nt) {
+__device__ __forceinline__ void unstage_plane(R* __restrict__ PRs, const R* __restrict__ SG, int PN, int PW, int SW,
+                                              int SN, const Consts<R>& K, R pfloor, int tid, int nt) {
     for (int c = tid; c < PN; c += nt) {
+        const int cs = (c / PW) * SW + c % PW + 2;
         Q9<R> q;
 #pragma unroll
-        for (int v = 0; v < 9; ++v) q.v[v] = SG[v * PN + c];
+        for (int v = 0; v < 9; ++v) q.v[v] = SG[v * SN + cs];
         q = cons2prim(q, K.gamma, K.smallr, pfloor);
 #pragma unroll
         for (int v = 0; v < 9; ++v) PRs[v * PN + c] = q.v[v];
     }
 }
 
-template <class R> __host__ __device__ inline size_t unsplit_smem_bytes(int ox, int oy) {
+// shared-memory layout of the tile march: PR ring, ST states, then (128-byte aligned, as a TMA
+// destination) the staging plane SG, then (16-byte aligned) the reduction and mbarrier words
+template <class R> __host__ __device__ inline size_t unsplit_sg_offset(int ox, int oy) {
     size_t PN = (size_t)(ox + 4) * (oy + 4), RN = (size_t)(ox + 2) * (oy + 2);
-    return (27 * PN + 36 * RN + 9 * PN) * sizeof(R) + 40 * sizeof(double);
+    return ((27 * PN + 36 * RN) * sizeof(R) + 127) / 128 * 128;
+}
+template <class R> __host__ __device__ inline size_t unsplit_red_offset(int ox, int oy) {
+    size_t SN = (size_t)(ox + 8) * (oy + 4);
+    return (unsplit_sg_offset<R>(ox, oy) + 9 * SN * sizeof(R) + 15) / 16 * 16;
+}
+template <class R> __host__ __device__ inline size_t unsplit_smem_bytes(int ox, int oy) {
+    return unsplit_red_offset<R>(ox, oy) + 40 * sizeof(double);
 }
 
 // The two schemes that share the tile march.  A scheme supplies the primitive floor of the
@@ -232,16 +246,19 @@ template <class R, int RECON> struct MarchScheme {
 // One tile (bx, by) x z-chunk bz of one box.  TOX, TOY > 0 fix the tile at compile time
 // (constant shared-memory offsets); 0 = runtime tile.  Used by the single-box kernel (one tile per
 // block) and by the ensemble kernel (a queue of tiles over many boxes).
-template <class R, class S, int TOX, int TOY, bool OVERHANG = false>
+// TMA: the kernel's A is a grid-constant parameter, so A.tmap can be handed to the TMA unit
+// (the ensemble kernel copies its arguments from global memory and keeps the cp.async path).
+template <class R, class S, int TOX, int TOY, bool OVERHANG = false, bool TMA = false>
 __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepVals<R>& V, int bx, int by, int bz,
                                             unsigned char* smem_raw) {
     const int OX = TOX > 0 ? TOX : A.ox, OY = TOY > 0 ? TOY : A.oy;
     const int PW = OX + 4, PN = (OX + 4) * (OY + 4);
     const int RW = OX + 2, RN = (OX + 2) * (OY + 2);
+    const int SW = OX + 8, SN = (OX + 8) * (OY + 4);
     R* PR = reinterpret_cast<R*>(smem_raw);
     R* ST = PR + 27 * PN;
-    R* SG = ST + 36 * RN;
-    double* red = reinterpret_cast<double*>(SG + 9 * PN);
+    R* SG = reinterpret_cast<R*>(smem_raw + unsplit_sg_offset<R>(OX, OY));
+    double* red = reinterpret_cast<double*>(smem_raw + unsplit_red_offset<R>(OX, OY));
 
     const int tid = threadIdx.x, NT = OX * OY;
     const int tx = tid % OX, ty = tid / OX;
@@ -260,14 +277,28 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     const int stg0 = NT - hwarp >= 32 ? hwarp : 0;                 // first staging thread
     const int nunst = NT - bwarp >= 32 ? NT - bwarp : NT;          // unstaging threads [0, nunst)
 
+    // a tile whose staged region (x0-4 .. x0+OX+3, y0-2 .. y0+OY+1) lies inside the box stages its
+    // planes by one TMA copy each (the tensor map addresses no periodic images); the others, and
+    // every tile when the caller supplied no map, by per-thread cp.async
+    bool tma = false;
+    if constexpr (TMA) {
+        tma = A.use_tma && x0 >= 4 && x0 + OX + 4 <= nx && y0 >= 2 && y0 + OY + 2 <= ny;
+        // a TMA destination must be 128-byte aligned; otherwise stay on cp.async
+        if ((unsigned)__cvta_generic_to_shared(SG) & 127u) tma = false;
+    }
+    const unsigned tma_bytes = (unsigned)(9 * SN * sizeof(R));
+
     // prologue: primitives of planes z0-2, z0-1, z0
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
     for (int j = 0; j < 3; ++j) {
-        stage_plane(SG, A.u, PN, PW, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
+        stage_plane(SG, A.u, PN, PW, SW, SN, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
         cp_async_wait_all();
         __syncthreads();
-        unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, SG, PN, K, S::prim_floor(K), tid, NT);
-        if (j == 2 && tid == 0) mbar_init(mbar, NT);
+        unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, SG, PN, PW, SW, SN, K, S::prim_floor(K), tid, NT);
+        if (j == 2 && tid == 0) {
+            mbar_init(mbar, tma ? 1u : (unsigned)NT);
+            if (tma) fence_mbar_init();
+        }
         __syncthreads();
     }
 
@@ -300,8 +331,20 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
         const bool load = kr + 2 <= z1 + 1;
         const int s0 = mod3(kr), sm = mod3(kr - 1), sp = mod3(kr + 1);
         if (load) {
-            stage_plane(SG, A.u, PN, PW, x0, y0, kr + 2, nx, ny, nz, tid >= stg0 ? tid - stg0 : PN, NT - stg0);
-            mbar_arrive_cp_async(mbar);
+            if constexpr (TMA) {
+                if (tma) {
+                    if (tid == 0) {
+                        fence_proxy_async_smem();   // the previous plane's reads of SG come first
+                        mbar_arrive_expect_tx(mbar, tma_bytes);
+                        tma_load_4d(SG, &A.tmap, x0 - 4, y0 - 2, wrapi(kr + 2, nz), 0, mbar);
+                    }
+                }
+            }
+            if (!tma) {
+                stage_plane(SG, A.u, PN, PW, SW, SN, x0, y0, kr + 2, nx, ny, nz, tid >= stg0 ? tid - stg0 : PN,
+                            NT - stg0);
+                mbar_arrive_cp_async(mbar);
+            }
         }
         {
             Q9<R> XY;
@@ -410,7 +453,8 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
         if (load) {
             mbar_wait(mbar, phase, A.err);
             phase ^= 1u;
-            unstage_plane(PR + mod3(kr + 2) * 9 * PN, SG, PN, K, S::prim_floor(K), tid < nunst ? tid : PN, nunst);
+            unstage_plane(PR + mod3(kr + 2) * 9 * PN, SG, PN, PW, SW, SN, K, S::prim_floor(K), tid < nunst ? tid : PN,
+                          nunst);
         }
         __syncthreads();
     }
@@ -422,10 +466,10 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     }
 }
 
-template <class R, int RECON, int RIEM, int TOX, int TOY, bool OVERHANG = false>
+template <class R, int RECON, int RIEM, int TOX, int TOY, bool OVERHANG = false, bool TMA = false>
 __device__ __forceinline__ void unsplit_tile(const UnsplitArgs<R>& A, const StepVals<R>& V, int bx, int by, int bz,
                                              unsigned char* smem_raw) {
-    scheme_tile<R, UnsplitScheme<R, RECON, RIEM>, TOX, TOY, OVERHANG>(A, V, bx, by, bz, smem_raw);
+    scheme_tile<R, UnsplitScheme<R, RECON, RIEM>, TOX, TOY, OVERHANG, TMA>(A, V, bx, by, bz, smem_raw);
 }
 
 // A tile = (box, bx, by, bz) work item of the ensemble kernel.
@@ -437,7 +481,7 @@ template <class R, int RECON, int RIEM, int TOX, int TOY, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) ensemble_kernel(const UnsplitArgs<R>* __restrict__ boxes,
                                                               const EnsItem* __restrict__ items, int nitems,
                                                               unsigned* queue) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ int item_s;
     for (;;) {
         if (threadIdx.x == 0) item_s = (int)atomicAdd(queue, 1u);
@@ -453,16 +497,18 @@ __global__ void __launch_bounds__(MAXT, MINB) ensemble_kernel(const UnsplitArgs<
 }
 
 template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0>
-__global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const UnsplitArgs<R> A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    unsplit_tile<R, RECON, RIEM, TOX, TOY>(A, step_vals(A), blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+__global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const __grid_constant__ UnsplitArgs<R> A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsplit_tile<R, RECON, RIEM, TOX, TOY, false, std::is_same<R, float>::value>(A, step_vals(A), blockIdx.x, blockIdx.y,
+                                                                                 blockIdx.z, smem_raw);
 }
 
 // Tiled march step (the scheme behind march_run_dev); RECON is RECON_MC or RECON_PPM.
 template <class R, int RECON, int MAXT, int MINB, int TOX = 0, int TOY = 0>
-__global__ void __launch_bounds__(MAXT, MINB) march_tile_kernel(const UnsplitArgs<R> A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    scheme_tile<R, MarchScheme<R, RECON>, TOX, TOY>(A, step_vals(A), blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+__global__ void __launch_bounds__(MAXT, MINB) march_tile_kernel(const __grid_constant__ UnsplitArgs<R> A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    scheme_tile<R, MarchScheme<R, RECON>, TOX, TOY, false, std::is_same<R, float>::value>(
+        A, step_vals(A), blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 }  // namespace gmt
