@@ -96,6 +96,9 @@ struct gmt_ctx {
     struct TmaMap { const void* base; CUtensorMap map; };
     TmaMap tma[2] = {};            // tensor maps of the last two input states (FP32 tile staging)
     int tma_next = 0;
+    struct CtTmaMap { const void* base; CUtensorMap map8, map1; };
+    CtTmaMap ct_tma[2] = {};       // the same for the CT state (8 variables, and bzf alone)
+    int ct_tma_next = 0;
 };
 
 namespace {
@@ -168,38 +171,78 @@ EncodeTiledFn encode_tiled_fn() {
 // (plane stride nx*ny*nz), 16-byte aligned, with nx and the tile width multiples of 4 (16-byte
 // rows and box origins): a 4-D map (x, y, z, variable) whose box is the tile's staged region,
 // (ox+8) x (oy+4) x 1 plane x 9 variables.  Otherwise use_tma stays 0 and every tile uses cp.async.
+// a 4-D FP32 map (x, y, z, variable) of nvar planes of nx*ny*nz cells from base, box
+// bx x by x 1 x bv; false if it cannot be made (then the caller stages by cp.async)
+bool encode_state_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, int nvar, int bx, int by, int bv) {
+    EncodeTiledFn enc = encode_tiled_fn();
+    if (!enc) return false;
+    const size_t n = (size_t)nx * ny * nz;
+    const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nvar};
+    const cuuint64_t strides[3] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4, (cuuint64_t)n * 4};
+    const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)bv};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the TMA preconditions shared by both tile marches: one array of nvar planes, 16-byte aligned,
+// nx and the tile width multiples of 4, box extents within 256 and the grid at least one box
+template <class P> const float* tma_base(const P& planes, int nvar, int nx, int ny, int nz, int ox, int oy, int rows) {
+    if (nx % 4 != 0 || ox % 4 != 0 || ox + 8 > 256 || oy + rows > 256 || nx < ox + 8 || ny < oy + rows) return nullptr;
+    const size_t n = (size_t)nx * ny * nz;
+    const float* base = reinterpret_cast<const float*>(planes.p[0]);
+    for (int v = 1; v < nvar; ++v)
+        if (reinterpret_cast<const float*>(planes.p[v]) != base + (size_t)v * n) return nullptr;
+    if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return nullptr;
+    return base;
+}
+
 template <class R> void set_tma(gmt_ctx* c, UnsplitArgs<R>& A) {
     A.use_tma = 0;
     std::memset(&A.tmap, 0, sizeof(A.tmap));
     if (sizeof(R) != 4) return;
-    const int nx = A.nx, ny = A.ny, nz = A.nz, ox = A.ox, oy = A.oy;
-    if (nx % 4 != 0 || ox % 4 != 0 || ox + 8 > 256 || oy + 4 > 256 || nx < ox + 8 || ny < oy + 4) return;
-    const size_t n = (size_t)nx * ny * nz;
-    const R* base = A.u.p[0];
-    for (int v = 1; v < 9; ++v)
-        if (A.u.p[v] != base + (size_t)v * n) return;
-    if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return;
+    const float* base = tma_base(A.u, 9, A.nx, A.ny, A.nz, A.ox, A.oy, 4);
+    if (!base) return;
     for (const gmt_ctx::TmaMap& t : c->tma)
         if (t.base == base) {
             A.tmap = t.map;
             A.use_tma = 1;
             return;
         }
-    EncodeTiledFn enc = encode_tiled_fn();
-    if (!enc) return;
     CUtensorMap m;
-    const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, 9};
-    const cuuint64_t strides[3] = {(cuuint64_t)nx * sizeof(R), (cuuint64_t)nx * ny * sizeof(R), (cuuint64_t)n * sizeof(R)};
-    const cuuint32_t box[4] = {(cuuint32_t)(ox + 8), (cuuint32_t)(oy + 4), 1, 9};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<R*>(base), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return;
+    if (!encode_state_map(&m, base, A.nx, A.ny, A.nz, 9, A.ox + 8, A.oy + 4, 9)) return;
     c->tma[c->tma_next].base = base;
     c->tma[c->tma_next].map = m;
     c->tma_next ^= 1;
     A.tmap = m;
+    A.use_tma = 1;
+}
+
+// CT: the staged region is (ox+8) x (oy+5) cells; one map moves the 8 state variables, one bzf
+template <class R> void set_ct_tma(gmt_ctx* c, CTArgs<R>& A) {
+    A.use_tma = 0;
+    std::memset(&A.tmap8, 0, sizeof(A.tmap8));
+    std::memset(&A.tmap1, 0, sizeof(A.tmap1));
+    if (sizeof(R) != 4) return;
+    const float* base = tma_base(A.q, 8, A.nx, A.ny, A.nz, A.ox, A.oy, 5);
+    if (!base) return;
+    for (const gmt_ctx::CtTmaMap& t : c->ct_tma)
+        if (t.base == base) {
+            A.tmap8 = t.map8;
+            A.tmap1 = t.map1;
+            A.use_tma = 1;
+            return;
+        }
+    CUtensorMap m8, m1;
+    if (!encode_state_map(&m8, base, A.nx, A.ny, A.nz, 8, A.ox + 8, A.oy + 5, 8)) return;
+    if (!encode_state_map(&m1, base, A.nx, A.ny, A.nz, 8, A.ox + 8, A.oy + 5, 1)) return;
+    c->ct_tma[c->ct_tma_next].base = base;
+    c->ct_tma[c->ct_tma_next].map8 = m8;
+    c->ct_tma[c->ct_tma_next].map1 = m1;
+    c->ct_tma_next ^= 1;
+    A.tmap8 = m8;
+    A.tmap1 = m1;
     A.use_tma = 1;
 }
 
@@ -337,6 +380,7 @@ int ct_step_impl(gmt_ctx* c, const CPlanes8<R>& q, const Planes8<R>& o, const gm
     A.trigx = static_cast<const R*>(c->trig[0]);
     A.scratch = static_cast<R*>(c->ct_scratch);
     A.err = c->err;
+    set_ct_tma(c, A);
     cudaError_t e = launch_ct(A, s);
     if (e != cudaSuccess) return cuda_fail(e, "ct step");
     if (a->want_cfl) {

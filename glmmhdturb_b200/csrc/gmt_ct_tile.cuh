@@ -45,27 +45,35 @@ enum CTScratch {
 };
 
 // byte offset of the reduction / mbarrier words: after the real arrays, rounded up to 16 bytes
+// staging plane: 128-byte aligned (a TMA destination), after the rings and the states
+template <class R> __host__ __device__ inline size_t ct_tile_sg_offset(int ox, int oy) {
+    size_t PN = (size_t)(ox + 4) * (oy + 4), RN = (size_t)(ox + 2) * (oy + 2);
+    return ((27 * PN + 9 * PN + 36 * RN) * sizeof(R) + 127) / 128 * 128;
+}
 template <class R> __host__ __device__ inline size_t ct_tile_words_offset(int ox, int oy) {
-    size_t PN = (size_t)(ox + 4) * (oy + 4), RN = (size_t)(ox + 2) * (oy + 2), PN5 = (size_t)(ox + 5) * (oy + 5);
-    return ((27 * PN + 9 * PN + 36 * RN + 9 * PN5) * sizeof(R) + 15) / 16 * 16;
+    size_t SN5 = (size_t)(ox + 8) * (oy + 5);
+    return (ct_tile_sg_offset<R>(ox, oy) + 9 * SN5 * sizeof(R) + 15) / 16 * 16;
 }
 template <class R> __host__ __device__ inline size_t ct_tile_smem_bytes(int ox, int oy) {
     return ct_tile_words_offset<R>(ox, oy) + 40 * sizeof(double);
 }
 
 // stage plane kp: the conserved cell variables, the three face fields at kp and bzf at kp+1, on
-// the region x0-2..x0+OX+2, y0-2..y0+OY+2
+// the region x0-2..x0+OX+2, y0-2..y0+OY+2.  SG rows have the pitch SW = OX + 8 and the region
+// starts at column 2: the layout of the TMA box (x0-4, y0-2) of (OX+8) x (OY+5) cells.
 template <class R>
-__device__ __forceinline__ void ct_stage_plane(R* __restrict__ SG, const CPlanes8<R>& q, int PN5, int PW5, int x0,
-                                               int y0, int kp, int nx, int ny, int nz, int tid, int nt) {
+__device__ __forceinline__ void ct_stage_plane(R* __restrict__ SG, const CPlanes8<R>& q, int PN5, int PW5, int SW,
+                                               int SN5, int x0, int y0, int kp, int nx, int ny, int nz, int tid,
+                                               int nt) {
     const size_t gz = (size_t)wrapi(kp, nz), gz1 = (size_t)wrapi(kp + 1, nz);
     for (int c = tid; c < PN5; c += nt) {
         const int lx = c % PW5, ly = c / PW5;
         const size_t gxy = (size_t)wrapi(x0 - 2 + lx, nx) + (size_t)nx * wrapi(y0 - 2 + ly, ny);
         const size_t g = gxy + (size_t)nx * ny * gz, g1 = gxy + (size_t)nx * ny * gz1;
+        const int cs = ly * SW + lx + 2;
 #pragma unroll
-        for (int v = 0; v < 8; ++v) cp_async_r(SG + v * PN5 + c, q.p[v] + g);
-        cp_async_r(SG + 8 * PN5 + c, q.p[7] + g1);
+        for (int v = 0; v < 8; ++v) cp_async_r(SG + v * SN5 + cs, q.p[v] + g);
+        cp_async_r(SG + 8 * SN5 + cs, q.p[7] + g1);
     }
     cp_async_commit();
 }
@@ -73,17 +81,17 @@ __device__ __forceinline__ void ct_stage_plane(R* __restrict__ SG, const CPlanes
 // staged plane -> primitives with the face-averaged field (ct_mhd.jl:85-97) and the lower faces
 template <class R>
 __device__ __forceinline__ void ct_unstage_plane(R* __restrict__ PRs, R* __restrict__ FBs, const R* __restrict__ SG,
-                                                 int PN, int PW, int PN5, int PW5, const Consts<R>& K, int tid, int nt) {
+                                                 int PN, int PW, int SN5, int SW, const Consts<R>& K, int tid, int nt) {
     for (int c = tid; c < PN; c += nt) {
         const int lx = c % PW, ly = c / PW;
-        const int c5 = lx + PW5 * ly;
+        const int c5 = ly * SW + lx + 2;
         Q9<R> cu;
 #pragma unroll
-        for (int v = 0; v < 5; ++v) cu.v[v] = SG[v * PN5 + c5];
-        const R bxl = SG[5 * PN5 + c5], byl = SG[6 * PN5 + c5], bzl = SG[7 * PN5 + c5];
-        cu.v[5] = R(0.5) * (bxl + SG[5 * PN5 + c5 + 1]);
-        cu.v[6] = R(0.5) * (byl + SG[6 * PN5 + c5 + PW5]);
-        cu.v[7] = R(0.5) * (bzl + SG[8 * PN5 + c5]);
+        for (int v = 0; v < 5; ++v) cu.v[v] = SG[v * SN5 + c5];
+        const R bxl = SG[5 * SN5 + c5], byl = SG[6 * SN5 + c5], bzl = SG[7 * SN5 + c5];
+        cu.v[5] = R(0.5) * (bxl + SG[5 * SN5 + c5 + 1]);
+        cu.v[6] = R(0.5) * (byl + SG[6 * SN5 + c5 + SW]);
+        cu.v[7] = R(0.5) * (bzl + SG[8 * SN5 + c5]);
         cu.v[8] = R(0);
         const Q9<R> q = cons2prim(cu, K.gamma, K.smallr, K.smallp);
 #pragma unroll
@@ -159,11 +167,12 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
     const int OX = TOX > 0 ? TOX : A.ox, OY = TOY > 0 ? TOY : A.oy;
     const int PW = OX + 4, PN = (OX + 4) * (OY + 4);
     const int PW5 = OX + 5, PN5 = (OX + 5) * (OY + 5);
+    const int SW = OX + 8, SN5 = (OX + 8) * (OY + 5);
     const int RW = OX + 2, RN = (OX + 2) * (OY + 2);
     R* PR = reinterpret_cast<R*>(smem_raw);
     R* FB = PR + 27 * PN;
     R* ST = FB + 9 * PN;
-    R* SG = ST + 36 * RN;
+    R* SG = reinterpret_cast<R*>(smem_raw + ct_tile_sg_offset<R>(OX, OY));
     double* red = reinterpret_cast<double*>(smem_raw + ct_tile_words_offset<R>(OX, OY));
 
     const int tid = threadIdx.x, NT = OX * OY;
@@ -183,14 +192,26 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
     const int nunst = NT - bwarp >= 32 ? NT - bwarp : NT;
     R* S = A.scratch;
 
+    // TMA staging (FP32, tiles whose region x0-4 .. x0+OX+3, y0-2 .. y0+OY+2 lies inside the box):
+    // one copy of the 8 state variables of plane k+2 and one of bzf at k+3 per plane
+    bool tma = false;
+    if constexpr (std::is_same<R, float>::value) {
+        tma = A.use_tma && x0 >= 4 && x0 + OX + 4 <= nx && y0 >= 2 && y0 + OY + 3 <= ny;
+        if ((unsigned)__cvta_generic_to_shared(SG) & 127u) tma = false;
+    }
+    const unsigned tma_bytes = (unsigned)(9 * SN5 * sizeof(R));
+
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
     for (int j = 0; j < 3; ++j) {
-        ct_stage_plane(SG, A.q, PN5, PW5, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
+        ct_stage_plane(SG, A.q, PN5, PW5, SW, SN5, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
         cp_async_wait_all();
         __syncthreads();
-        ct_unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, FB + mod3(z0 - 2 + j) * 3 * PN, SG, PN, PW, PN5, PW5, K, tid,
+        ct_unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, FB + mod3(z0 - 2 + j) * 3 * PN, SG, PN, PW, SN5, SW, K, tid,
                          NT);
-        if (j == 2 && tid == 0) mbar_init(mbar, NT);
+        if (j == 2 && tid == 0) {
+            mbar_init(mbar, tma ? 1u : (unsigned)NT);
+            if (tma) fence_mbar_init();
+        }
         __syncthreads();
     }
 
@@ -210,8 +231,19 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
         const int s0 = mod3(kr), sm = mod3(kr - 1), sp = mod3(kr + 1);
         const R* FB0 = FB + (size_t)s0 * 3 * PN;
         if (load) {
-            ct_stage_plane(SG, A.q, PN5, PW5, x0, y0, kr + 2, nx, ny, nz, tid >= stg0 ? tid - stg0 : PN5, NT - stg0);
-            mbar_arrive_cp_async(mbar);
+            if constexpr (std::is_same<R, float>::value) {
+                if (tma && tid == 0) {
+                    fence_proxy_async_smem();   // the previous plane's reads of SG come first
+                    mbar_arrive_expect_tx(mbar, tma_bytes);
+                    tma_load_4d(SG, &A.tmap8, x0 - 4, y0 - 2, wrapi(kr + 2, nz), 0, mbar);
+                    tma_load_4d(SG + 8 * SN5, &A.tmap1, x0 - 4, y0 - 2, wrapi(kr + 3, nz), 7, mbar);
+                }
+            }
+            if (!tma) {
+                ct_stage_plane(SG, A.q, PN5, PW5, SW, SN5, x0, y0, kr + 2, nx, ny, nz, tid >= stg0 ? tid - stg0 : PN5,
+                               NT - stg0);
+                mbar_arrive_cp_async(mbar);
+            }
         }
         {
             Q9<R> XY, Fxl, Fyl;
@@ -326,7 +358,7 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
         if (load) {
             mbar_wait(mbar, phase, A.err);
             phase ^= 1u;
-            ct_unstage_plane(PR + mod3(kr + 2) * 9 * PN, FB + mod3(kr + 2) * 3 * PN, SG, PN, PW, PN5, PW5, K,
+            ct_unstage_plane(PR + mod3(kr + 2) * 9 * PN, FB + mod3(kr + 2) * 3 * PN, SG, PN, PW, SN5, SW, K,
                              tid < nunst ? tid : PN, nunst);
         }
         __syncthreads();
@@ -335,8 +367,8 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
 }
 
 template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0>
-__global__ void __launch_bounds__(MAXT, MINB) ct_tile_kernel(const CTArgs<R> A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(MAXT, MINB) ct_tile_kernel(const __grid_constant__ CTArgs<R> A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     ct_tile<R, RECON, RIEM, TOX, TOY>(A, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 

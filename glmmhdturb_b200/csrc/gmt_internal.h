@@ -61,6 +61,9 @@ template <class R> struct CTArgs {
     const R* trigx;
     R* scratch;            // 15 planes: lower-face EMF data and cell EMFs (12), edge EMFs (3)
     int* err;              // device flag set when a bounded wait gives up
+    int use_tma;           // tmap8/tmap1 describe q: tiles clear of the box edges stage by TMA
+    CUtensorMap tmap8;     // 4-D map (x, y, z, variable) of q, box (ox+8) x (oy+5) x 1 x 8
+    CUtensorMap tmap1;     // the same tensor, box (ox+8) x (oy+5) x 1 x 1 (bzf of the next plane)
 };
 cudaError_t launch_ct(const CTArgs<float>& A, cudaStream_t s);
 cudaError_t launch_ct(const CTArgs<double>& A, cudaStream_t s);
