@@ -6,8 +6,9 @@
 //   PR[3][9][(OX+4)(OY+4)]  cell primitives with the face-averaged field (ring of 3 planes),
 //   FB[3][3][(OX+4)(OY+4)]  the lower-face fields bxf, byf, bzf of the same cells,
 //   ST[4][9][(OX+2)(OY+2)]  in-plane interface states, overwritten by the face fluxes,
-//   SG[9][(OX+5)(OY+5)]     staging of plane k+2: 5 conserved, bxf, byf, bzf(k+2), bzf(k+3)
-// (one more row and column than the ring, for the face averages of the outermost cells).  Per
+//   SG[9][(OY+5)][OX+8]     staging of plane k+2: 5 conserved, bxf, byf, bzf(k+2), bzf(k+3)
+// (one more row and column than the ring, for the face averages of the outermost cells, at column
+// offset 2; FP32 tiles clear of the box edges fill it by two TMA copies, the others by cp.async).  Per
 // direction each cell gets a full (or ct_mhd.jl's half) MonCen slope, the transverse-free 1-D
 // Hancock predictor and its two face states, whose normal component is the face field; every
 // face is solved once (HLL or HLLD, no GLM).  The write-out does the hydro update with the

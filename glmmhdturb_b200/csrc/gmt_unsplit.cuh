@@ -6,11 +6,13 @@
 //   PR[3][9][(OX+4)(OY+4)]  primitive ring (planes k-1, k, k+1; 2-cell in-plane halo),
 //   ST[4][9][(OX+2)(OY+2)]  in-plane interface states +x,-x,+y,-y of the reconstruction region,
 //                           overwritten in place by the face fluxes,
-//   SG[9][(OX+4)(OY+4)]     conserved staging plane k+2, filled by cp.async while plane k computes.
+//   SG[9][(OY+4)][OX+8]     conserved staging plane k+2 (the ring region at column offset 2),
+//                           filled while plane k computes.
 // Each owned thread keeps its column's z-face work in registers (the +z state of plane k-1 and
 // F_z at its lower face) plus its own x/y face fluxes, so every face is solved once, every cell is
 // read from HBM once and written once, and a plane costs two block barriers.  The next conserved
-// plane streams in by cp.async and completes on an mbarrier (bounded wait, error flag).
+// plane streams in by one TMA copy (FP32 tiles clear of the box edges) or by per-thread cp.async,
+// and completes on an mbarrier (bounded wait, error flag).
 //
 // Reference semantics: integrator_tiled!/integrator_plm!/integrator_plm_ppm!
 // (glmmhd_turb.jl:608-743, 782-864, 931-1014) -- one reconstruction per cell, one Riemann solve
