@@ -125,17 +125,19 @@ def test_ct_run_legacy_abi(golden):
     assert L.ct_regs() > 0
 
 
+@pytest.mark.parametrize("n", [16, 96])
 @pytest.mark.parametrize("recon", ["mc", "ppm"])
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
-def test_march_passive_species_vs_oracle(oracle, recon, dtype):
+def test_march_passive_species_vs_oracle(oracle, recon, dtype, n):
     """Two passive species on the march scheme (CMA, spike_mhd.cu NSP): FP64 bit-exact against the
-    oracle, FP32 within 1e-5 of it; the MHD planes match the species-free (tiled) step."""
+    oracle, FP32 within 1e-5 of it; the MHD planes match the species-free (tiled) step; at 16^3
+    and at 96^3 (three 32-column tiles of the step, periodic wrap of the 5-point species stencils)."""
     import math
     import numpy as np
     from glmmhdturb_b200 import Solver
     from tests.gpu_util import to_dev
     from tests.test_oracle import _march_species_state
-    n, nsp = 16, 2
+    nsp = 2
     cfg, u, u9 = _march_species_state(oracle, n, nsp, 7)
     cfg.recon = recon
     cfg9 = oracle.Config(n=(n, n, n), gamma=5 / 3, recon=recon, riemann="hll")
