@@ -463,6 +463,7 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     c->esize = p->dtype == GMT_F64 ? 8 : 4;
     c->n = (size_t)p->nx * p->ny * p->nz;
     cudaGetDevice(&c->device);
+    if (c->esize == 4) (void)encode_tiled_fn();   // the driver entry point, looked up outside any capture
     int rc = GMT_OK;
     if (p->scheme == GMT_SCHEME_UNSPLIT || p->scheme == GMT_SCHEME_MARCH1D) rc = choose_tile(c);
     if (p->scheme == GMT_SCHEME_CT) rc = choose_tile(c, true);
