@@ -190,4 +190,44 @@ def dot(a: torch.Tensor, b: torch.Tensor) -> float:
 
 
 __all__ = ["Schedule", "StepRecord", "StepFunction", "forward", "replay", "backward", "ke_band_gradient",
-           "checkpoint_interval", "velocity_b_direction", "adjoint_scratch_bytes", "dot"]
+           "checkpoint_interval", "velocity_b_direction", "adjoint_scratch_bytes", "dot", "step_cost"]
+
+
+def step_cost(n: int, dtype: str = "f32", reps: int = 10) -> dict:
+    """Device time of one forward step and of one adjoint step on the same seeded turbulent state
+    (PLM-MC + HLLD + GLM + forcing, CUDA events, after 3 warm-up calls): the adjoint cost ratio."""
+    s = Solver(n, dtype=dtype, gamma=5.0 / 3.0, turb_amp=2.0, turb_T=0.5, turb_seed=1, courant=0.3)
+    u = s.alloc()
+    s.ic_turbulent(u, mach=1.0, seed=1)
+    s.forcing_reset()
+    s.forcing_advance()
+    w = torch.empty_like(u)
+    g = torch.randn_like(u)
+    gb = torch.empty_like(u)
+    cm, sm = s.cfl(u)
+    dt = s.params.courant * s.dx / cm
+    fac = s.glm_fac(sm, dt)
+    calls = {"forward": lambda: s.step(u, w, dt, t=0.1, ch=sm, glm_fac=fac, do_turb=True),
+             "adjoint": lambda: s.adjoint_step(u, g, gb, dt, t=0.1, ch=sm, glm_fac=fac, do_turb=True)}
+    out = {}
+    for name, f in calls.items():
+        for _ in range(3):
+            f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        out[name + "_ms"] = e0.elapsed_time(e1) / reps
+    out["ratio"] = out["adjoint_ms"] / out["forward_ms"]
+    return out
+
+
+if __name__ == "__main__":   # python -m glmmhdturb_b200.adjoint [n] [f32|f64]
+    import sys
+    n = int(sys.argv[1]) if len(sys.argv) > 1 else 128
+    dt_name = sys.argv[2] if len(sys.argv) > 2 else "f32"
+    r = step_cost(n, dt_name)
+    print(f"{n}^3 {dt_name}: forward {r['forward_ms']:.3f} ms, adjoint {r['adjoint_ms']:.3f} ms, ratio {r['ratio']:.2f}")

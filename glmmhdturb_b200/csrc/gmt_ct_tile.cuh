@@ -380,18 +380,21 @@ template <class R> __device__ __forceinline__ R ct_upwind(R flux, R minus, R plu
 // Pass B1: the three edge EMFs of cell (i,j,k) -- ez at (i-1/2, j-1/2, k), ex at (i, j-1/2, k-1/2),
 // ey at (i-1/2, j, k-1/2) -- for the cyclic axes (A, B, e): on the A-face the face EMF is
 // -F_A[B_B], on the B-face +F_B[B_A]; the same expressions and order as the oracle.
-template <class R> __global__ void __launch_bounds__(256) ct_edge_kernel(const CTArgs<R> A) {
+// All loads of a cell come first and all stores after them, so that a thread keeps its loads in
+// flight together (the stores go to other scratch planes than the loads read).
+template <class R, bool CONTACT> __global__ void __launch_bounds__(256) ct_edge_kernel(const CTArgs<R> A) {
     const int nx = A.nx, ny = A.ny, nz = A.nz;
     const size_t n = (size_t)nx * ny * nz;
     const R* S = A.scratch;
     R* W = A.scratch;
-    const bool contact = A.emf == 1;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
         int x, y, z;
         cell_coords(c, nx, ny, n, x, y, z);
         const size_t xm = (size_t)wrap1(x - 1, nx) + (size_t)nx * (y + (size_t)ny * z);
         const size_t ym = (size_t)x + (size_t)nx * (wrap1(y - 1, ny) + (size_t)ny * z);
         const size_t zm = (size_t)x + (size_t)nx * (y + (size_t)ny * wrap1(z - 1, nz));
+        // per edge e: EaN, EaS, EbE, EbW, then (contact) e00, e10, e01, e11, maN, maS, mbE, mbW
+        R v[3][12];
 #pragma unroll
         for (int e = 0; e < 3; ++e) {
             // A = (e+1)%3, B = (e+2)%3; c10 = one step back along A, c01 along B, c11 along both
@@ -410,15 +413,31 @@ template <class R> __global__ void __launch_bounds__(256) ct_edge_kernel(const C
                 c11 = (size_t)wrap1(x - 1, nx) + (size_t)nx * (y + (size_t)ny * wrap1(z - 1, nz));
                 ea = CS_EYZ; eb = CS_EYX; ma = CS_MZ; mb = CS_MX; ec = CS_ECY;
             }
-            const R EaN = S[ea * n + c], EaS = S[ea * n + c01];
-            const R EbE = S[eb * n + c], EbW = S[eb * n + c10];
+            v[e][0] = S[ea * n + c];
+            v[e][1] = S[ea * n + c01];
+            v[e][2] = S[eb * n + c];
+            v[e][3] = S[eb * n + c10];
+            if (CONTACT) {
+                v[e][4] = S[ec * n + c];
+                v[e][5] = S[ec * n + c10];
+                v[e][6] = S[ec * n + c01];
+                v[e][7] = S[ec * n + c11];
+                v[e][8] = S[ma * n + c];
+                v[e][9] = S[ma * n + c01];
+                v[e][10] = S[mb * n + c];
+                v[e][11] = S[mb * n + c10];
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            const R EaN = v[e][0], EaS = v[e][1], EbE = v[e][2], EbW = v[e][3];
             R E = R(0.25) * (EbE + EbW + EaN + EaS);
-            if (contact) {
-                const R e00 = S[ec * n + c], e10 = S[ec * n + c10], e01 = S[ec * n + c01], e11 = S[ec * n + c11];
-                const R dN = ct_upwind(S[ma * n + c], e10 - EbW, e00 - EbE);
-                const R dS = ct_upwind(S[ma * n + c01], EbW - e11, EbE - e01);
-                const R dE = ct_upwind(S[mb * n + c], e01 - EaS, e00 - EaN);
-                const R dW = ct_upwind(S[mb * n + c10], EaS - e11, EaN - e10);
+            if (CONTACT) {
+                const R e00 = v[e][4], e10 = v[e][5], e01 = v[e][6], e11 = v[e][7];
+                const R dN = ct_upwind(v[e][8], e10 - EbW, e00 - EbE);
+                const R dS = ct_upwind(v[e][9], EbW - e11, EbE - e01);
+                const R dE = ct_upwind(v[e][10], e01 - EaS, e00 - EaN);
+                const R dW = ct_upwind(v[e][11], EaS - e11, EaN - e10);
                 E = E + R(0.25) * (dS - dN) + R(0.25) * (dW - dE);
             }
             W[(CS_EDX + e) * n + c] = E;
@@ -440,9 +459,13 @@ template <class R> __global__ void __launch_bounds__(256) ct_face_kernel(const C
         const size_t cxp = (size_t)wrap1(x + 1, nx) + (size_t)nx * (y + (size_t)ny * z);
         const size_t cyp = (size_t)x + (size_t)nx * (wrap1(y + 1, ny) + (size_t)ny * z);
         const size_t czp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrap1(z + 1, nz));
-        A.o.p[5][c] = A.q.p[5][c] - dtdx * ((ez[cyp] - ez[c]) - (ey[czp] - ey[c]));
-        A.o.p[6][c] = A.q.p[6][c] - dtdx * ((ex[czp] - ex[c]) - (ez[cxp] - ez[c]));
-        A.o.p[7][c] = A.q.p[7][c] - dtdx * ((ey[cxp] - ey[c]) - (ex[cyp] - ex[c]));
+        // every load before the first store (the outputs may share an allocation with the inputs)
+        const R exc = ex[c], eyc = ey[c], ezc = ez[c];
+        const R ezy = ez[cyp], eyz = ey[czp], exz = ex[czp], ezx = ez[cxp], eyx = ey[cxp], exy = ex[cyp];
+        const R b5 = A.q.p[5][c], b6 = A.q.p[6][c], b7 = A.q.p[7][c];
+        A.o.p[5][c] = b5 - dtdx * ((ezy - ezc) - (eyz - eyc));
+        A.o.p[6][c] = b6 - dtdx * ((exz - exc) - (ezx - ezc));
+        A.o.p[7][c] = b7 - dtdx * ((eyx - eyc) - (exy - exc));
     }
 }
 
@@ -462,7 +485,8 @@ static cudaError_t ct_go(const CTArgs<R>& A, cudaStream_t s, bool configure_only
     k<<<grid, nt, ct_tile_smem_bytes<R>(A.ox, A.oy), s>>>(A);
     const size_t n = (size_t)A.nx * A.ny * A.nz;
     const int nb = (int)std::min<size_t>((n + 255) / 256, (size_t)148 * 16);
-    ct_edge_kernel<R><<<nb, 256, 0, s>>>(A);
+    if (A.emf == 1) ct_edge_kernel<R, true><<<nb, 256, 0, s>>>(A);
+    else ct_edge_kernel<R, false><<<nb, 256, 0, s>>>(A);
     ct_face_kernel<R><<<nb, 256, 0, s>>>(A);
     return cudaGetLastError();
 }
