@@ -216,16 +216,27 @@ def test_ct_turbulent_state_is_divergence_free(dtype):
     assert s.ct_divb_max(q) <= 10 * tol and bool(torch.isfinite(q).all())
 
 
+def _misaligned_like(u0):
+    """A float32 copy of u0 whose base address is 4 bytes past a 16-byte boundary: the library
+    cannot describe it by a tensor map, so every tile stages by cp.async."""
+    big = torch.empty(u0.size + 1, dtype=torch.float32, device="cuda")
+    q = big[1:].view(u0.shape)
+    q.copy_(torch.from_numpy(np.ascontiguousarray(u0)).float())
+    return q
+
+
 @pytest.mark.parametrize("scheme,recon,riem", [("unsplit", "mc", "hlld"), ("unsplit", "ppm", "hll"),
                                                ("march1d", "mc", "hll"), ("ct", "mc", "hlld"), ("ct", "ppm", "hll")])
 def test_fp32_production_tile_vs_oracle(oracle, scheme, recon, riem):
     """The FP32 step kernels specialised at compile time for the 32x16 production tile (the shape
-    the autotuner picks at 512^3) against the FP64 oracle on a 64x32x16 grid, three steps, and
-    against the same FP32 step on a runtime 16x16 tile."""
+    the autotuner picks at 512^3) against the FP64 oracle on a 128x128x16 grid, three steps; the
+    same step with every tile staged by cp.async (a misaligned state) bit for bit; and the same
+    FP32 step on a runtime 16x16 tile.  At this size the 32x16 tiles clear of the box edges stage
+    by TMA and the others by cp.async."""
     import math
     from glmmhdturb_b200 import Solver
     from tests.gpu_util import perturbed_glm_state
-    n = (64, 32, 16)
+    n = (128, 128, 16)
     if scheme == "ct":
         cfg = oracle.Config(n=n, gamma=5 / 3, recon=recon, riemann=riem, emf="contact")
         u0 = oracle.ct_ic_ot(cfg)
@@ -240,11 +251,14 @@ def test_fp32_production_tile_vs_oracle(oracle, scheme, recon, riem):
     if scheme == "march1d":
         kw["smallp"] = cfg.smallp
     outs = {}
-    for tile in ((32, 16, 0), (16, 16, 0)):
+    for tile, misaligned in (((32, 16, 0), False), ((32, 16, 0), True), ((16, 16, 0), False)):
         s = Solver(n, tile=tile, **kw)
         assert s.kernel_info()["tile"][:2] == tile[:2]
-        q = to_dev(u0, torch.float32)
-        w = torch.empty_like(q)
+        if misaligned:
+            q, w = _misaligned_like(u0), _misaligned_like(u0)
+        else:
+            q = to_dev(u0, torch.float32)
+            w = torch.empty_like(q)
         ref = u0
         for _ in range(3):
             if scheme == "ct":
@@ -264,10 +278,15 @@ def test_fp32_production_tile_vs_oracle(oracle, scheme, recon, riem):
             q, w = w, q
         got = q.cpu().numpy()
         err, errs = max_rel_err(got, ref)
-        # the 8 MHD fields to FP32 round-off; the GLM psi is a small field sourced by round-off
-        assert max(errs[:8]) <= 3e-5, (tile, errs)
+        rel2 = [float(np.linalg.norm(got[v] - ref[v]) / max(np.linalg.norm(ref[v]), 1e-300)) for v in range(8)]
+        # the 8 MHD fields to FP32 round-off in the L2 norm; pointwise, a discrete switch (PPM's
+        # pressure-jump fallback, a limiter branch) that flips between FP32 and FP64 at a few cells
+        # leaves a larger local difference
+        assert max(rel2) <= 1e-5 and max(errs[:8]) <= 1e-3, (tile, misaligned, errs, rel2)
         if scheme != "ct":
-            assert errs[8] <= 1e-2, (tile, errs)
-        outs[tile] = got
-    err, errs = max_rel_err(outs[(32, 16, 0)], outs[(16, 16, 0)].astype(np.float64))
+            assert errs[8] <= 1e-2, (tile, misaligned, errs)
+        outs[(tile, misaligned)] = got
+    # TMA staging and cp.async staging deliver the same bytes
+    np.testing.assert_array_equal(outs[((32, 16, 0), False)], outs[((32, 16, 0), True)])
+    err, errs = max_rel_err(outs[((32, 16, 0), False)], outs[((16, 16, 0), False)].astype(np.float64))
     assert max(errs[:8]) <= 1e-5, errs
