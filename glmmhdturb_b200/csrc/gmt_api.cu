@@ -94,7 +94,7 @@ struct gmt_ctx {
     void* adj = nullptr;           // adjoint scratch (207 planes, allocated on first use)
     double* adj_damp = nullptr;    // dL/d(turb_amp) accumulator
     struct TmaMap { const void* base; CUtensorMap map; };
-    TmaMap tma[2] = {};            // tensor maps of the last two input states (FP32 tile staging)
+    TmaMap tma[2] = {};            // tensor maps of the last two input states (tile staging)
     int tma_next = 0;
     struct CtTmaMap { const void* base; CUtensorMap map8, map1; };
     CtTmaMap ct_tma[2] = {};       // the same for the CT state (8 variables, and bzf alone)
@@ -167,33 +167,37 @@ EncodeTiledFn encode_tiled_fn() {
     return fn;
 }
 
-// The FP32 tile march stages its planes by TMA when the input state is one array of 9 planes
+// The tile marches stage their planes by TMA when the input state is one array of its planes
 // (plane stride nx*ny*nz), 16-byte aligned, with nx and the tile width multiples of 4 (16-byte
-// rows and box origins): a 4-D map (x, y, z, variable) whose box is the tile's staged region,
-// (ox+8) x (oy+4) x 1 plane x 9 variables.  Otherwise use_tma stays 0 and every tile uses cp.async.
-// a 4-D FP32 map (x, y, z, variable) of nvar planes of nx*ny*nz cells from base, box
-// bx x by x 1 x bv; false if it cannot be made (then the caller stages by cp.async)
-bool encode_state_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, int nvar, int bx, int by, int bv) {
+// rows and box origins in either precision): a 4-D map (x, y, z, variable) whose box is the tile's
+// staged region, (ox+8) x (oy+4 or 5) x 1 plane x the variables.  Otherwise use_tma stays 0 and
+// every tile uses cp.async.
+// a 4-D map (x, y, z, variable) of nvar planes of nx*ny*nz reals from base, box bx x by x 1 x bv;
+// false if it cannot be made (then the caller stages by cp.async)
+template <class R>
+bool encode_state_map(CUtensorMap* m, const R* base, int nx, int ny, int nz, int nvar, int bx, int by, int bv) {
     EncodeTiledFn enc = encode_tiled_fn();
     if (!enc) return false;
-    const size_t n = (size_t)nx * ny * nz;
+    const size_t n = (size_t)nx * ny * nz, es = sizeof(R);
     const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nvar};
-    const cuuint64_t strides[3] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4, (cuuint64_t)n * 4};
+    const cuuint64_t strides[3] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es, (cuuint64_t)n * es};
     const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)bv};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(base), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+    const CUtensorMapDataType dt = es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    return enc(m, dt, 4, const_cast<R*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // the TMA preconditions shared by both tile marches: one array of nvar planes, 16-byte aligned,
 // nx and the tile width multiples of 4, box extents within 256 and the grid at least one box
-template <class P> const float* tma_base(const P& planes, int nvar, int nx, int ny, int nz, int ox, int oy, int rows) {
+template <class R, class P>
+const R* tma_base(const P& planes, int nvar, int nx, int ny, int nz, int ox, int oy, int rows) {
     if (nx % 4 != 0 || ox % 4 != 0 || ox + 8 > 256 || oy + rows > 256 || nx < ox + 8 || ny < oy + rows) return nullptr;
     const size_t n = (size_t)nx * ny * nz;
-    const float* base = reinterpret_cast<const float*>(planes.p[0]);
+    const R* base = planes.p[0];
     for (int v = 1; v < nvar; ++v)
-        if (reinterpret_cast<const float*>(planes.p[v]) != base + (size_t)v * n) return nullptr;
+        if (planes.p[v] != base + (size_t)v * n) return nullptr;
     if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return nullptr;
     return base;
 }
@@ -201,8 +205,7 @@ template <class P> const float* tma_base(const P& planes, int nvar, int nx, int 
 template <class R> void set_tma(gmt_ctx* c, UnsplitArgs<R>& A) {
     A.use_tma = 0;
     std::memset(&A.tmap, 0, sizeof(A.tmap));
-    if (sizeof(R) != 4) return;
-    const float* base = tma_base(A.u, 9, A.nx, A.ny, A.nz, A.ox, A.oy, 4);
+    const R* base = tma_base<R>(A.u, 9, A.nx, A.ny, A.nz, A.ox, A.oy, 4);
     if (!base) return;
     for (const gmt_ctx::TmaMap& t : c->tma)
         if (t.base == base) {
@@ -224,8 +227,7 @@ template <class R> void set_ct_tma(gmt_ctx* c, CTArgs<R>& A) {
     A.use_tma = 0;
     std::memset(&A.tmap8, 0, sizeof(A.tmap8));
     std::memset(&A.tmap1, 0, sizeof(A.tmap1));
-    if (sizeof(R) != 4) return;
-    const float* base = tma_base(A.q, 8, A.nx, A.ny, A.nz, A.ox, A.oy, 5);
+    const R* base = tma_base<R>(A.q, 8, A.nx, A.ny, A.nz, A.ox, A.oy, 5);
     if (!base) return;
     for (const gmt_ctx::CtTmaMap& t : c->ct_tma)
         if (t.base == base) {
@@ -463,7 +465,7 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
     c->esize = p->dtype == GMT_F64 ? 8 : 4;
     c->n = (size_t)p->nx * p->ny * p->nz;
     cudaGetDevice(&c->device);
-    if (c->esize == 4) (void)encode_tiled_fn();   // the driver entry point, looked up outside any capture
+    (void)encode_tiled_fn();   // the driver entry point, looked up outside any capture
     int rc = GMT_OK;
     if (p->scheme == GMT_SCHEME_UNSPLIT || p->scheme == GMT_SCHEME_MARCH1D) rc = choose_tile(c);
     if (p->scheme == GMT_SCHEME_CT) rc = choose_tile(c, true);

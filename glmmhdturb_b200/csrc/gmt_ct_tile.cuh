@@ -8,7 +8,7 @@
 //   ST[4][9][(OX+2)(OY+2)]  in-plane interface states, overwritten by the face fluxes,
 //   SG[9][(OY+5)][OX+8]     staging of plane k+2: 5 conserved, bxf, byf, bzf(k+2), bzf(k+3)
 // (one more row and column than the ring, for the face averages of the outermost cells, at column
-// offset 2; FP32 tiles clear of the box edges fill it by two TMA copies, the others by cp.async).  Per
+// offset 2; tiles clear of the box edges fill it by two TMA copies, the others by cp.async).  Per
 // direction each cell gets a full (or ct_mhd.jl's half) MonCen slope, the transverse-free 1-D
 // Hancock predictor and its two face states, whose normal component is the face field; every
 // face is solved once (HLL or HLLD, no GLM).  The write-out does the hydro update with the
@@ -193,10 +193,10 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
     const int nunst = NT - bwarp >= 32 ? NT - bwarp : NT;
     R* S = A.scratch;
 
-    // TMA staging (FP32, tiles whose region x0-4 .. x0+OX+3, y0-2 .. y0+OY+2 lies inside the box):
+    // TMA staging (tiles whose region x0-4 .. x0+OX+3, y0-2 .. y0+OY+2 lies inside the box):
     // one copy of the 8 state variables of plane k+2 and one of bzf at k+3 per plane
     bool tma = false;
-    if constexpr (std::is_same<R, float>::value) {
+    {
         tma = A.use_tma && x0 >= 4 && x0 + OX + 4 <= nx && y0 >= 2 && y0 + OY + 3 <= ny;
         if ((unsigned)__cvta_generic_to_shared(SG) & 127u) tma = false;
     }
@@ -232,7 +232,7 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
         const int s0 = mod3(kr), sm = mod3(kr - 1), sp = mod3(kr + 1);
         const R* FB0 = FB + (size_t)s0 * 3 * PN;
         if (load) {
-            if constexpr (std::is_same<R, float>::value) {
+            {
                 if (tma && tid == 0) {
                     fence_proxy_async_smem();   // the previous plane's reads of SG come first
                     mbar_arrive_expect_tx(mbar, tma_bytes);

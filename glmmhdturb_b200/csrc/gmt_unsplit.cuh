@@ -11,7 +11,7 @@
 // Each owned thread keeps its column's z-face work in registers (the +z state of plane k-1 and
 // F_z at its lower face) plus its own x/y face fluxes, so every face is solved once, every cell is
 // read from HBM once and written once, and a plane costs two block barriers.  The next conserved
-// plane streams in by one TMA copy (FP32 tiles clear of the box edges) or by per-thread cp.async,
+// plane streams in by one TMA copy (tiles clear of the box edges) or by per-thread cp.async,
 // and completes on an mbarrier (bounded wait, error flag).
 //
 // Reference semantics: integrator_tiled!/integrator_plm!/integrator_plm_ppm!
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(MAXT, MINB) ensemble_kernel(const UnsplitArgs<
 template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0>
 __global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const __grid_constant__ UnsplitArgs<R> A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsplit_tile<R, RECON, RIEM, TOX, TOY, false, std::is_same<R, float>::value>(A, step_vals(A), blockIdx.x, blockIdx.y,
+    unsplit_tile<R, RECON, RIEM, TOX, TOY, false, true>(A, step_vals(A), blockIdx.x, blockIdx.y,
                                                                                  blockIdx.z, smem_raw);
 }
 
@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(MAXT, MINB) unsplit_kernel(const __grid_consta
 template <class R, int RECON, int MAXT, int MINB, int TOX = 0, int TOY = 0>
 __global__ void __launch_bounds__(MAXT, MINB) march_tile_kernel(const __grid_constant__ UnsplitArgs<R> A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    scheme_tile<R, MarchScheme<R, RECON>, TOX, TOY, false, std::is_same<R, float>::value>(
+    scheme_tile<R, MarchScheme<R, RECON>, TOX, TOY, false, true>(
         A, step_vals(A), blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 

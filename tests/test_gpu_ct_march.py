@@ -37,10 +37,10 @@ def test_golden(golden, case, dtype):
     assert err <= (1e-12 if dtype == "f64" else 3e-5), errs
 
 
+@pytest.mark.parametrize("n", [(24, 16, 12), (96, 40, 10)])   # the second has TMA-staged tiles
 @pytest.mark.parametrize("emf,riem", [("average", "hll"), ("contact", "hlld")])
-def test_ct_noncubic_vs_oracle_and_divb(oracle, emf, riem):
+def test_ct_noncubic_vs_oracle_and_divb(oracle, emf, riem, n):
     from glmmhdturb_b200 import Solver
-    n = (24, 16, 12)
     cfg = oracle.Config(n=n, gamma=5 / 3, riemann=riem, emf=emf)
     q0 = oracle.ct_ic_ot(cfg)
     rng = np.random.default_rng(3)
@@ -169,7 +169,8 @@ def test_march_passive_species_vs_oracle(oracle, recon, dtype, n):
 
 
 @pytest.mark.parametrize("recon", ["mc", "ppm"])
-@pytest.mark.parametrize("n,tile", [((32, 24, 20), (0, 0, 0)), ((32, 32, 16), (16, 8, 5)), ((24, 16, 12), (8, 16, 0))])
+@pytest.mark.parametrize("n,tile", [((32, 24, 20), (0, 0, 0)), ((32, 32, 16), (16, 8, 5)), ((24, 16, 12), (8, 16, 0)),
+                                    ((96, 40, 10), (32, 8, 0))])   # the last has TMA-staged tiles
 def test_tiled_march_vs_oracle(oracle, recon, n, tile):
     """The tiled march kernel (one solve per face, z-march) against the oracle on non-cubic grids,
     odd z-chunks and several tiles; FP64 bit-exact, and the fused CFL equals the oracle's."""

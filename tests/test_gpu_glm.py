@@ -41,7 +41,8 @@ def test_unsplit_golden(golden, case, dtype):
 
 
 @pytest.mark.parametrize("n,tile", [((32, 16, 12), (0, 0, 0)), ((24, 20, 10), (8, 4, 3)),
-                                    ((16, 16, 16), (16, 8, 5)), ((12, 8, 7), (4, 2, 2))])
+                                    ((16, 16, 16), (16, 8, 5)), ((12, 8, 7), (4, 2, 2)),
+                                    ((96, 40, 10), (32, 8, 5))])   # the last has TMA-staged tiles
 @pytest.mark.parametrize("recon,riem", [("mc", "hlld"), ("ppm", "hll")])
 def test_unsplit_tiles_vs_oracle(oracle, n, tile, recon, riem):
     from glmmhdturb_b200 import Solver
