@@ -4,5 +4,5 @@
 
 namespace gmt {
 size_t adjoint_scratch_reals(size_t n) { return (size_t)(54 + 27 + 9 + 54 + 63) * n; }
-template cudaError_t launch_adjoint<double>(const AdjArgs<double>&, cudaStream_t);
+template cudaError_t launch_adjoint<double>(const AdjArgs<double>&, const UnsplitArgs<double>*, cudaStream_t);
 }  // namespace gmt

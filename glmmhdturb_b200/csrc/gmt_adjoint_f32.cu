@@ -3,5 +3,5 @@
 #include "gmt_adjoint_kern.cuh"
 
 namespace gmt {
-template cudaError_t launch_adjoint<float>(const AdjArgs<float>&, cudaStream_t);
+template cudaError_t launch_adjoint<float>(const AdjArgs<float>&, const UnsplitArgs<float>*, cudaStream_t);
 }  // namespace gmt

@@ -772,7 +772,30 @@ int gmt_adjoint_step(gmt_ctx* c, const void* u, const void* ubar_next, void* uba
         A.FSb = A.R1b + 9 * c->n;
         A.QB = A.FSb + 54 * c->n;
         A.damp = c->adj_damp;
-        cudaError_t e = launch_adjoint<R>(A, s);
+        // passes 1-3 by the forward step's tile march in record mode (the context's tile)
+        UnsplitArgs<R> T;
+        T.u = A.u;
+        T.o = planes<R>(ubar, c->n);   // not written in record mode
+        T.nx = p.nx; T.ny = p.ny; T.nz = p.nz;
+        T.ox = c->ox; T.oy = c->oy; T.lz = c->lz;
+        T.dt = A.dt; T.dtdx = A.dtdx; T.ch = A.ch; T.glm_fac = A.glm_fac; T.ramp = A.ramp;
+        T.K = A.K;
+        T.iflo = A.iflo; T.use_llf = A.use_llf; T.do_turb = A.do_turb;
+        T.btab = A.btab; T.trigx = A.trigx;
+        T.cfl_out = nullptr;
+        T.err = c->err;
+        T.dx = (R)dx;
+        T.dparams = nullptr;
+        T.fmass = nullptr;
+        set_tma(c, T);
+        T.rec_fs = A.FS;
+        T.rec_ubn = A.ubn.p[0];
+        T.rec_r1b = A.R1b;
+        T.rec_ub = A.ub.p[0];
+        T.rec_damp = A.damp;
+        T.rec_amp = A.amp;
+        const bool record = c->ox > 0 && c->oy > 0 && c->lz > 0;
+        cudaError_t e = launch_adjoint<R>(A, record ? &T : nullptr, s);
         return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_adjoint_step");
     };
     return c->esize == 8 ? go(0.0) : go(0.0f);

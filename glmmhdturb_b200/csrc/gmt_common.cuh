@@ -39,6 +39,14 @@ template <class R> struct UnsplitArgs {
                            // for the passive-species pass of the march scheme
     int use_tma;           // tmap describes u: tiles clear of the box edges stage by TMA
     CUtensorMap tmap;      // 4-D map (x, y, z, variable) of u; box (ox+8) x (oy+4) x 1 x 9
+    // adjoint record mode (a scheme with kRecord): the step writes every cell's six interface
+    // states and, in place of the new state, the adjoint of its update epilogue
+    R* rec_fs;             // 54 planes: interface states +x, -x, +y, -y, +z, -z of every cell
+    const R* rec_ubn;      // 9 planes: adjoint of the step's output
+    R* rec_r1b;            // 9 planes: adjoint of the pre-epilogue state
+    R* rec_ub;             // 9 planes: adjoint of the step's input, identity part
+    double* rec_damp;      // dL/d(forcing amplitude) accumulator
+    R rec_amp;             // forcing amplitude
 };
 
 // step values of one box, from the kernel arguments or from device memory

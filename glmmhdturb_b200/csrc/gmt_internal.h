@@ -124,7 +124,8 @@ template <class R> struct AdjArgs {
     double* damp;          // dL/d(forcing amplitude) accumulator
 };
 size_t adjoint_scratch_reals(size_t n);
-template <class R> cudaError_t launch_adjoint(const AdjArgs<R>& A, cudaStream_t s);
+// rec: the forward step's tile arguments for the record tile (passes 1-3 in one march), or null
+template <class R> cudaError_t launch_adjoint(const AdjArgs<R>& A, const UnsplitArgs<R>* rec, cudaStream_t s);
 cudaError_t upload_mode_table();   // the 61 wavevectors into constant memory
 cudaError_t mode_table_device(const int** ptr);   // device address of that table
 void set_last_error(const std::string& msg);   // message returned by gmt_last_error() on this thread

@@ -146,6 +146,13 @@ template <class R> __host__ __device__ inline size_t unsplit_smem_bytes(int ox, 
     return unsplit_red_offset<R>(ox, oy) + 40 * sizeof(double);
 }
 
+// adjoint record mode: interface state k (+x, -x, +y, -y, +z, -z) of cell g
+template <class R> __device__ __forceinline__ void rec_put(const UnsplitArgs<R>& A, size_t n, int k, size_t g,
+                                                          const Q9<R>& f) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) A.rec_fs[(size_t)(k * 9 + v) * n + g] = f.v[v];
+}
+
 // The two schemes that share the tile march.  A scheme supplies the primitive floor of the
 // staged planes, the reconstruction of a cell (recon, then prep<D> before the states of
 // direction D), its interface states, the face flux and the update epilogue.
@@ -154,6 +161,7 @@ template <class R> __host__ __device__ inline size_t unsplit_smem_bytes(int ox, 
 // directions, iflo revert, HLLD/HLL/LLF + GLM, void floor, psi damping and forcing kick.
 template <class R, int RECON, int RIEM> struct UnsplitScheme {
     using Cell = Rec<R>;
+    static constexpr bool kRecord = false;   // adjoint record mode (AdjRecordScheme)
     static __device__ __forceinline__ R prim_floor(const Consts<R>& K) { return K.pfl; }
     static __device__ __forceinline__ void recon(const R* PR, int PN, int PW, int c, int s0, int sm, int sp,
                                                  const Consts<R>& K, R dtdx, Cell& r) {
@@ -187,6 +195,7 @@ template <class R> struct MarchCell {
 };
 template <class R, int RECON> struct MarchScheme {
     using Cell = MarchCell<R>;
+    static constexpr bool kRecord = false;
     static __device__ __forceinline__ R prim_floor(const Consts<R>& K) { return K.smallp; }
     static __device__ __forceinline__ void recon(const R* PR, int PN, int, int c, int s0, int, int, const Consts<R>&, R,
                                                  Cell& r) {
@@ -310,6 +319,7 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
 #pragma unroll
     for (int v = 0; v < 9; ++v) { pPz.v[v] = R(0); Fzlo.v[v] = R(0); Fxh.v[v] = R(0); Fyh.v[v] = R(0); }
     R cmax = R(0), smax = R(0);   // exact maxima in R, widened to FP64 once per block
+    double damp = 0.0;            // record mode: this thread's share of dL/d(forcing amplitude)
     // OVERHANG: a tile may overhang the box (an ensemble box narrower than a tile multiple); the
     // overhanging columns recompute the periodic images of cells at the start of the row, bit for
     // bit the same values, so their duplicate writes (and CFL maxima) are harmless
@@ -362,18 +372,43 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
             }
             typename S::Cell r;
             S::recon(PR, PN, PW, cown, s0, sm, sp, K, dtdx, r);
+            // the own cell of plane kr (a cell of this chunk when kr is neither first nor last)
+            const size_t gk = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * (size_t)(kr < 0 ? 0 : kr));
+            const size_t ncell = (size_t)nx * ny * nz;
             if (!first && !last) {
                 S::template prep<0>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx);
-                st_put(ST + 0 * 9 * RN, RN, rown, S::template state<0, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
-                st_put(ST + 1 * 9 * RN, RN, rown, S::template state<0, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+                {
+                    const Q9<R> f = S::template state<0, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+                    st_put(ST + 0 * 9 * RN, RN, rown, f);
+                    if constexpr (S::kRecord) rec_put(A, ncell, 0, gk, f);
+                }
+                {
+                    const Q9<R> f = S::template state<0, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+                    st_put(ST + 1 * 9 * RN, RN, rown, f);
+                    if constexpr (S::kRecord) rec_put(A, ncell, 1, gk, f);
+                }
                 S::template prep<1>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx);
-                st_put(ST + 2 * 9 * RN, RN, rown, S::template state<1, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
-                st_put(ST + 3 * 9 * RN, RN, rown, S::template state<1, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo));
+                {
+                    const Q9<R> f = S::template state<1, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+                    st_put(ST + 2 * 9 * RN, RN, rown, f);
+                    if constexpr (S::kRecord) rec_put(A, ncell, 2, gk, f);
+                }
+                {
+                    const Q9<R> f = S::template state<1, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+                    st_put(ST + 3 * 9 * RN, RN, rown, f);
+                    if constexpr (S::kRecord) rec_put(A, ncell, 3, gk, f);
+                }
             }
             S::template prep<2>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx);
             Q9<R> Pz = S::template state<2, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+            if constexpr (S::kRecord) {
+                if (!first && !last) rec_put(A, ncell, 4, gk, Pz);
+            }
             if (!first) {
                 Q9<R> Mz = S::template state<2, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
+                if constexpr (S::kRecord) {
+                    if (!last) rec_put(A, ncell, 5, gk, Mz);
+                }
                 Q9<R> Fzhi = S::template flux<2>(pPz, Mz, K, ch, A.use_llf != 0);
                 if (kr - 1 >= z0) {
                     const int kf = kr - 1;
@@ -383,20 +418,36 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
                     for (int v = 0; v < 9; ++v) q.v[v] = A.u.p[v][g] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
                     R ax = R(0), ay = R(0), az = R(0);
                     if (turb) force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
-                    S::finish(q, K, V.glm_fac, turb, ax, ay, az, V.dt);
+                    if constexpr (S::kRecord) {
+                        // the epilogue's adjoint at the pre-epilogue state q; R1bar and the identity
+                        // part of ubar, and this cell's share of dL/d(amplitude)
+                        Q9<R> ob, rb;
 #pragma unroll
-                    for (int v = 0; v < 9; ++v) A.o.p[v][g] = q.v[v];
-                    if (A.fmass) {
-                        const size_t nc = (size_t)nx * ny * nz;
-                        A.fmass[g] = fmx;
-                        A.fmass[nc + g] = fmy;
-                        A.fmass[2 * nc + g] = Fzlo.v[0];
-                    }
-                    if (A.cfl_out) {
-                        R ct, sg;
-                        cfl_speeds(q, K, ct, sg);
-                        cmax = fmax(cmax, ct);
-                        smax = fmax(smax, sg);
+                        for (int v = 0; v < 9; ++v) ob.v[v] = A.rec_ubn[(size_t)v * ncell + g];
+                        R ab[3];
+                        S::epilogue_adj(q, K, V.glm_fac, turb, ax, ay, az, V.dt, ob, rb, ab);
+#pragma unroll
+                        for (int v = 0; v < 9; ++v) {
+                            A.rec_r1b[(size_t)v * ncell + g] = rb.v[v];
+                            A.rec_ub[(size_t)v * ncell + g] = rb.v[v];
+                        }
+                        if (turb && A.rec_amp != R(0))
+                            damp += ((double)ab[0] * ax + (double)ab[1] * ay + (double)ab[2] * az) / (double)A.rec_amp;
+                    } else {
+                        S::finish(q, K, V.glm_fac, turb, ax, ay, az, V.dt);
+#pragma unroll
+                        for (int v = 0; v < 9; ++v) A.o.p[v][g] = q.v[v];
+                        if (A.fmass) {
+                            A.fmass[g] = fmx;
+                            A.fmass[ncell + g] = fmy;
+                            A.fmass[2 * ncell + g] = Fzlo.v[0];
+                        }
+                        if (A.cfl_out) {
+                            R ct, sg;
+                            cfl_speeds(q, K, ct, sg);
+                            cmax = fmax(cmax, ct);
+                            smax = fmax(smax, sg);
+                        }
                     }
                 }
                 Fzlo = Fzhi;
@@ -461,6 +512,21 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
         __syncthreads();
     }
     if (tid == 0) mbar_inval(mbar);
+    if constexpr (S::kRecord) {
+        // block sum of the amplitude partials (red[0..31]; the mbarrier word sits at red[32])
+        double v = damp;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((tid & 31) == 0) red[tid >> 5] = v;
+        __syncthreads();
+        if (tid < 32) {
+            double x = tid < (NT + 31) / 32 ? red[tid] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (tid == 0 && x != 0.0 && A.rec_damp) atomicAdd(A.rec_damp, x);
+        }
+        __syncthreads();   // red is free again for a following tile of the same block
+    } else {
+        (void)damp;
+    }
     if (A.cfl_out) {
         block_max_atomic((double)cmax, A.cfl_out, red);
         __syncthreads();
