@@ -27,6 +27,7 @@
 #include "gmt_oracle.h"
 
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -48,6 +49,15 @@ static int nthreads() {
 #else
     return 1;
 #endif
+}
+
+// Branch counters: how often each guarded branch of the reference fired since the last reset
+// (ORC_CNT_* in gmt_oracle.h).  A fixture that claims to exercise a branch asserts its count > 0.
+// Counting is off unless a caller switches it on, so the timed baseline pays one branch per site.
+static std::atomic<int> g_count_on{0};
+static std::atomic<long long> g_cnt[ORC_CNT_N];
+static inline void count(int i) {
+    if (g_count_on.load(std::memory_order_relaxed)) g_cnt[i].fetch_add(1, std::memory_order_relaxed);
 }
 
 // IEEE maxNum/minNum, the same semantics as CUDA fmax/fmin and Julia's @fastmath max/min
@@ -291,9 +301,10 @@ static inline V9<R> hlld_x(const V9<R>& L, const V9<R>& Rr, R gamma, R bn, R fbn
     R sqdLs = osqrt(dLs), sqdRs = osqrt(dRs);
     R SLs = SM - oabs(bn) / sqdLs;
     R SRs = SM + oabs(bn) / sqdRs;
-    auto star = [&](R d, R u, R v, R w, R by, R bz, R S, R& vy, R& vz, R& byS, R& bzS) {
+    auto star = [&](R d, R u, R v, R w, R by, R bz, R S, R& vy, R& vz, R& byS, R& bzS, bool& degen) {
         R denK = d * (S - u) * (S - SM) - bn * bn;
-        if (oabs(denK) < tiny) {
+        degen = oabs(denK) < tiny;   // degenerate star state (glmmhd_turb.jl:225-238)
+        if (degen) {
             vy = v; vz = w; byS = by; bzS = bz;
         } else {
             R fac = bn * (SM - u) / denK;
@@ -304,8 +315,9 @@ static inline V9<R> hlld_x(const V9<R>& L, const V9<R>& Rr, R gamma, R bn, R fbn
         }
     };
     R vyLs, vzLs, byLs, bzLs, vyRs, vzRs, byRs, bzRs;
-    star(dL, uL, vL, wL, byL, bzL, SL, vyLs, vzLs, byLs, bzLs);
-    star(dR, uR, vR, wR, byR, bzR, SR, vyRs, vzRs, byRs, bzRs);
+    bool degL, degR;
+    star(dL, uL, vL, wL, byL, bzL, SL, vyLs, vzLs, byLs, bzLs, degL);
+    star(dR, uR, vR, wR, byR, bzR, SR, vyRs, vzRs, byRs, bzRs, degR);
     R vdotbL = uL * bn + vL * byL + wL * bzL;
     R vdotbLs = SM * bn + vyLs * byLs + vzLs * bzLs;
     R ELs = ((SL - uL) * EL - ptL * uL + pts * SM + bn * (vdotbL - vdotbLs)) / (SL - SM);
@@ -326,14 +338,23 @@ static inline V9<R> hlld_x(const V9<R>& L, const V9<R>& Rr, R gamma, R bn, R fbn
     V9<R> ULss = {dLs, dLs * SM, dLs * vyss, dLs * vzss, ELss, bn, byss, bzss, R(0)};
     V9<R> URss = {dRs, dRs * SM, dRs * vyss, dRs * vzss, ERss, bn, byss, bzss, R(0)};
     V9<R> f;
+    // sampling (glmmhd_turb.jl:262-270); a degenerate star counts when the region uses it
     if (SLs >= R(0)) {
         for (int i = 0; i < 9; ++i) f[i] = FL[i] + SL * (ULs[i] - UL[i]);
+        count(ORC_CNT_HLLD_L);
+        if (degL) count(ORC_CNT_HLLD_DEGEN);
     } else if (SM >= R(0)) {
         for (int i = 0; i < 9; ++i) f[i] = FL[i] + SLs * ULss[i] - (SLs - SL) * ULs[i] - SL * UL[i];
+        count(ORC_CNT_HLLD_LS);
+        if (degL || degR) count(ORC_CNT_HLLD_DEGEN);
     } else if (SRs >= R(0)) {
         for (int i = 0; i < 9; ++i) f[i] = FR[i] + SRs * URss[i] - (SRs - SR) * URs[i] - SR * UR[i];
+        count(ORC_CNT_HLLD_RS);
+        if (degL || degR) count(ORC_CNT_HLLD_DEGEN);
     } else {
         for (int i = 0; i < 9; ++i) f[i] = FR[i] + SR * (URs[i] - UR[i]);
+        count(ORC_CNT_HLLD_R);
+        if (degR) count(ORC_CNT_HLLD_DEGEN);
     }
     f[5] = fbn; f[8] = fpsi;
     return f;
@@ -355,8 +376,10 @@ static inline V9<R> riemann(const V9<R>& Lq, const V9<R>& Rq, int d, const Phys<
     } else if (P.riemann == ORC_RIEMANN_LLF_BOUND) {
         f = llf_x(L, Rr, P.gamma, ch, fbn, fpsi, true);
     } else {
-        bool uself = (P.llf_dmin > R(0) && rmin(L[0], Rr[0]) < P.llf_dmin) ||
-                     (P.llf_pmin > R(0) && rmin(L[4], Rr[4]) < P.llf_pmin) || P.riemann == ORC_RIEMANN_LLF;
+        bool sw = (P.llf_dmin > R(0) && rmin(L[0], Rr[0]) < P.llf_dmin) ||
+                  (P.llf_pmin > R(0) && rmin(L[4], Rr[4]) < P.llf_pmin);   // glmmhd_turb.jl:287-289
+        if (sw && P.riemann == ORC_RIEMANN_HLLD) count(ORC_CNT_LLF_SWITCH);
+        bool uself = sw || P.riemann == ORC_RIEMANN_LLF;
         f = uself ? llf_x(L, Rr, P.gamma, ch, fbn, fpsi, false) : hlld_x(L, Rr, P.gamma, bns, fbn, fpsi);
     }
     return rot_from(f, d);
@@ -509,9 +532,10 @@ template <class R> static inline V9<R> load9(const R* u, const Grid& g, int i, i
 // (glmmhd_turb.jl:447-475 with the tiled kernel's sc2 = smallc^2 grouping, :849-858)
 template <class R>
 static inline V9<R> finish_update(V9<R> r1, const Phys<R>& P, R glm_fac, bool turb, const R acc[3], R dt) {
-    if (r1[0] < P.smallr) {
+    if (r1[0] < P.smallr) {   // void floor (glmmhd_turb.jl:450-453)
         R emag = R(0.5) * (r1[5] * r1[5] + r1[6] * r1[6] + r1[7] * r1[7]);
         r1 = {P.smallr, R(0), R(0), R(0), P.pfl / (P.gamma - R(1)) + emag, r1[5], r1[6], r1[7], r1[8]};
+        count(ORC_CNT_VOID_FLOOR);
     }
     V9<R> r = r1;
     r[8] = r1[8] * glm_fac;
@@ -550,12 +574,16 @@ static inline Faces<R> recon_cell(const R* u, const Grid& g, int i, int j, int k
     bool mm = P.recon == ORC_RECON_MINMOD;
     V9<R> sx = slope(mxl, m0, mxr, mm), sy = slope(myl, m0, myr, mm), sz = slope(mzl, m0, mzr, mm);
     V9<R> mh = cons2prim(hancock(m0, sx, sy, sz, dtdx, P.gamma), P.gamma, P.smallr, P.pfl);
-    if (mh[0] <= P.smallr || mh[4] <= P.pfl) mh = m0;
+    if (mh[0] <= P.smallr || mh[4] <= P.pfl) {   // predictor revert (glmmhd_turb.jl:393-395)
+        mh = m0;
+        count(ORC_CNT_HANCOCK_REVERT);
+    }
     Faces<R> F;
     const V9<R>* s[3] = {&sx, &sy, &sz};
     if (P.recon == ORC_RECON_PPM) {
         // integrator_plm_ppm! stage 2 (glmmhd_turb.jl:952-975)
         bool up = !(spj(mxl[4], m0[4], mxr[4]) || spj(myl[4], m0[4], myr[4]) || spj(mzl[4], m0[4], mzr[4]));
+        if (!up) count(ORC_CNT_PPM_FALLBACK);
         const V9<R>* nb[3][2] = {{&mxl, &mxr}, {&myl, &myr}, {&mzl, &mzr}};
         for (int d = 0; d < 3; ++d) {
             if (up) {
@@ -578,7 +606,10 @@ static inline Faces<R> recon_cell(const R* u, const Grid& g, int i, int j, int k
     }
     if (P.iflo)
         for (int f = 0; f < 6; ++f)
-            if (F.f[f][0] < P.smallr || F.f[f][4] < P.pfl) F.f[f] = m0;
+            if (F.f[f][0] < P.smallr || F.f[f][4] < P.pfl) {   // iflo revert (glmmhd_turb.jl:618)
+                F.f[f] = m0;
+                count(ORC_CNT_IFLO_REVERT);
+            }
     return F;
 }
 
@@ -675,7 +706,9 @@ static inline V9<R> hanc1d(const V9<R>& c0, const V9<R>& s, int d, R dtdx, R gam
     V9<R> U = prim2cons(c0, gamma);
     R h = R(0.5) * dtdx;
     for (int v = 0; v < 9; ++v) U[v] = U[v] - h * (FR[v] - FL[v]);
-    return prim_from_cons_floor(U, gamma, smallr, smallp);
+    V9<R> q = prim_from_cons_floor(U, gamma, smallr, smallp);
+    if (q[0] <= smallr || q[4] <= smallp) count(ORC_CNT_PRED1D_FLOOR);   // floored predictor
+    return q;
 }
 // spike moncen(a,b,c) = sgn*min(|dc|, 2|dl|, 2|dr|), dc = (c-a)/2  (full slope)
 template <class R> static inline R full_mc(R a, R b, R c) {
@@ -710,6 +743,7 @@ static inline V9<R> march_face(const V9<R>& m2, const V9<R>& m1, const V9<R>& c0
         L = padd(mhL, sL, R(0.5));
         Rr = padd(mhR, sR, R(-0.5));
     }
+    if (L[0] < P.smallr || L[4] < P.smallp || Rr[0] < P.smallr || Rr[4] < P.smallp) count(ORC_CNT_FACE_FLOOR);
     L[0] = rmax(L[0], P.smallr); L[4] = rmax(L[4], P.smallp);
     Rr[0] = rmax(Rr[0], P.smallr); Rr[4] = rmax(Rr[4], P.smallp);
     // hllMHD (spike_mhd.cu:199-223) == riemann_hll with the floors already applied
@@ -849,6 +883,7 @@ static inline V9<R> ct_face_flux(const V9<R>& m2, const V9<R>& m1, const V9<R>& 
         L = padd(mhL, sL, R(0.5));
         Rr = padd(mhR, sR, R(-0.5));
     }
+    if (L[0] < P.smallr || L[4] < P.smallp || Rr[0] < P.smallr || Rr[4] < P.smallp) count(ORC_CNT_FACE_FLOOR);
     L[0] = rmax(L[0], P.smallr); L[4] = rmax(L[4], P.smallp);
     Rr[0] = rmax(Rr[0], P.smallr); Rr[4] = rmax(Rr[4], P.smallp);
     L[5 + d] = bn; Rr[5 + d] = bn;
@@ -1057,6 +1092,14 @@ template <class R> static void diag(const orc_params* p, const R* u, orc_diag* d
 extern "C" {
 
 int orc_set_threads(int n) { g_threads = n; return nthreads(); }
+void orc_count_reset(int on) {
+    g_count_on.store(0);
+    for (auto& c : g_cnt) c.store(0);
+    g_count_on.store(on ? 1 : 0);
+}
+void orc_count_get(int64_t* out, int n) {
+    for (int i = 0; i < n && i < ORC_CNT_N; ++i) out[i] = (int64_t)g_cnt[i].load();
+}
 int orc_num_modes(void) { return modes_table().n; }
 void orc_mode_k(int32_t* k3) {
     const ModeTable& t = modes_table();

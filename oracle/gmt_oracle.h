@@ -24,6 +24,23 @@ enum { ORC_RIEMANN_HLLD = 0, ORC_RIEMANN_HLL = 1, ORC_RIEMANN_LLF = 2, ORC_RIEMA
 enum { ORC_EMF_AVERAGE = 0, ORC_EMF_CONTACT = 1 };
 #define ORC_NMODES 61
 
+/* branch counters (orc_count_reset / orc_count_get): each guarded branch of the reference */
+enum {
+    ORC_CNT_HANCOCK_REVERT = 0, /* unsplit predictor rho <= smallr or p <= pfl -> m0 (glmmhd_turb.jl:393-395) */
+    ORC_CNT_IFLO_REVERT,        /* interface state rho < smallr or p < pfl -> m0 (glmmhd_turb.jl:618) */
+    ORC_CNT_VOID_FLOOR,         /* updated rho < smallr -> void state (glmmhd_turb.jl:450-453) */
+    ORC_CNT_LLF_SWITCH,         /* HLLD face switched to LLF by llf_dmin / llf_pmin (glmmhd_turb.jl:287-289) */
+    ORC_CNT_HLLD_DEGEN,         /* |denK| < 1e-12 star state used by the sampled region (glmmhd_turb.jl:225-238) */
+    ORC_CNT_HLLD_L,             /* HLLD sampled region: F_L* (SL* >= 0) */
+    ORC_CNT_HLLD_LS,            /* F_L** (SL* < 0 <= SM) */
+    ORC_CNT_HLLD_RS,            /* F_R** (SM < 0 <= SR*) */
+    ORC_CNT_HLLD_R,             /* F_R* (SR* < 0) */
+    ORC_CNT_PPM_FALLBACK,       /* PPM cell falls back to PLM faces on a pressure jump (spj, glmmhd_turb.jl:952-975) */
+    ORC_CNT_FACE_FLOOR,         /* march / CT face state floored at smallr / smallp (spike_mhd.cu:199-223) */
+    ORC_CNT_PRED1D_FLOOR,       /* march / CT 1-D predictor floored (spike_mhd.cu:149-161) */
+    ORC_CNT_N
+};
+
 typedef struct orc_params {
     int32_t nx, ny, nz;
     int32_t recon;      /* ORC_RECON_* */
@@ -55,6 +72,10 @@ typedef struct orc_diag {
 } orc_diag;
 
 int  orc_set_threads(int n);
+/* zero the branch counters and switch counting on (on != 0) or off */
+void orc_count_reset(int on);
+/* copy min(n, ORC_CNT_N) counters to out */
+void orc_count_get(int64_t* out, int n);
 int  orc_num_modes(void);
 void orc_mode_k(int32_t* k3);                   /* 3*ORC_NMODES ints */
 void orc_trig_table(int n, double* out);        /* [4 m][2 (cos,sin)][n] */

@@ -92,12 +92,40 @@ def lib():
         L.orc_ic_ot_f64.argtypes = [P, dp]
         L.orc_ic_uniform_f64.argtypes = [P] + [C.c_double] * 5 + [dp]
         L.orc_ct_ic_ot_f64.argtypes = [P, dp]
+        L.orc_count_reset.argtypes = [C.c_int]
+        L.orc_count_get.argtypes = [np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS"), C.c_int]
         _lib = L
     return _lib
 
 
 def set_threads(n: int) -> int:
     return lib().orc_set_threads(int(n))
+
+
+# names of the branch counters, in the order of ORC_CNT_* (gmt_oracle.h)
+COUNTERS = ("hancock_revert", "iflo_revert", "void_floor", "llf_switch", "hlld_degen", "hlld_L", "hlld_Ls",
+            "hlld_Rs", "hlld_R", "ppm_fallback", "face_floor", "pred1d_floor")
+
+
+class branch_counts:
+    """Context manager: count how often each guarded branch of the reference fires inside it.
+
+        with branch_counts() as bc:
+            step_unsplit(...)
+        bc.counts["void_floor"] > 0
+    """
+
+    def __enter__(self):
+        lib().orc_count_reset(1)
+        self.counts = {}
+        return self
+
+    def __exit__(self, *exc):
+        out = np.zeros(len(COUNTERS), dtype=np.int64)
+        lib().orc_count_get(out, len(COUNTERS))
+        lib().orc_count_reset(0)
+        self.counts = dict(zip(COUNTERS, (int(v) for v in out)))
+        return False
 
 
 @dataclass

@@ -206,3 +206,50 @@ def test_march_species_cma_properties(oracle, recon):
     out = O.step_march1d(cfg, u, dt, smax, 0.98)
     X = out[9] / np.maximum(out[0], cfg.smallr)
     assert np.abs(X - 0.3).max() <= 1e-13
+
+
+# ---------------------------------------------------------------------------------------------
+# Edge-case fixtures: every guarded branch of the reference fires in the committed fixture
+# ---------------------------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def edge():
+    import os
+    return dict(np.load(os.path.join(os.path.dirname(G.__file__), "edge_16x16x8.npz")))
+
+
+def test_edge_fixture_states_are_regenerated_exactly(edge):
+    assert np.array_equal(G.edge_state(G.EDGE_N), edge["glm_in"])
+    assert np.array_equal(G.ct_edge_state(G.EDGE_N), edge["ct_in"])
+    assert np.array_equal(np.array(G.edge_dt(G.EDGE_N)), edge["scalars"][[0, 1, 2, 5]])
+
+
+@pytest.mark.parametrize("case", G.EDGE_CASES, ids=[c[0] for c in G.EDGE_CASES])
+def test_edge_golden_and_branch_counts(oracle, edge, case):
+    """The oracle reproduces each committed edge-case step bit for bit, with the same branch
+    counts, and every branch the case is built for fires at least once."""
+    dt, ch, fac, _, _, ct_dt = edge["scalars"]
+    src = edge["ct_in"] if case[1] == "ct" else edge["glm_in"]
+    out, counts = G.edge_step(case, src, dt, ch, fac, ct_dt, edge["modes"])
+    assert np.array_equal(out, edge[case[0]])
+    assert [counts[k] for k in oracle.COUNTERS] == list(edge[case[0] + "__counts"])
+    for br in case[8]:
+        assert counts[br] > 0, (case[0], br, counts)
+    assert np.isfinite(out).all()
+    cdiv = oracle.ct_divb_max(G.edge_cfg(case), out) if case[1] == "ct" else 0.0
+    assert cdiv < 1e-12
+
+
+def test_edge_iflo_changes_the_step(edge):
+    # with the interface-state revert on, the step differs from the one without it
+    a, b = edge["edge_mc_hlld"], edge["edge_mc_hlld_noiflo"]
+    assert np.abs(a - b).max() > 1e-6
+
+
+def test_branch_counts_zero_on_a_smooth_state(oracle, golden):
+    # the smooth 8^3 fixture state triggers none of the revert / floor branches
+    cfg = oracle.Config(n=G.N, gamma=G.GAMMA, recon="mc", riemann="hlld", iflo=True)
+    with oracle.branch_counts() as bc:
+        oracle.step_unsplit(cfg, golden["glm_in"], G.DT, G.CH, G.FAC)
+    for k in ("hancock_revert", "iflo_revert", "void_floor", "llf_switch", "hlld_degen"):
+        assert bc.counts[k] == 0, (k, bc.counts)
+    assert sum(bc.counts[k] for k in ("hlld_L", "hlld_Ls", "hlld_Rs", "hlld_R")) >= 3 * 512
