@@ -366,7 +366,119 @@ GMT_HD void hlld_star(R d, R u, R v, R w, R by, R bz, R S, R SM, R bn, R& vy, R&
     }
 }
 
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000) && defined(GMT_PACKED_F32)
+// FP32 HLLD for the fast build: the same Miyoshi-Kusano states, sampled with fewer operations.
+//  - The sampled region lies on the side of the sign of SM in all four regions (SL* >= 0 implies
+//    SM >= 0, SR* < 0 implies SM < 0), so one side's star state is formed, and the other side's only
+//    for the double-star regions.
+//  - Every region's flux equals the physical flux of its sampled state with normal velocity SM and
+//    total pressure pT* (F_L + S_L (U*_L - U_L) = F(U*_L) and F*_L + S*_L (U**_L - U*_L) = F(U**_L)
+//    hold exactly in exact arithmetic, S_L clamped or not, since the star states solve those jump
+//    conditions; pT* = pT_L + rho_L (S_L - u_L)(SM - u_L) equals the symmetric form used here), so
+//    the flux is one evaluation F(rho*, SM, v*, w*, B*, E*, pT*) instead of F_side + S (U* - U).
+//    In the degenerate star branch (|denK| < 1e-12, where B_t vanishes) F(U*)[B_t] and the jump
+//    form differ by B_t (SM - u), which is zero with B_t.
+//  - The reciprocals of rho, of the HLL denominator and of S - SM are formed once.
+__device__ __forceinline__ Q9<float> hlld_x_f32(const Q9<float>& L, const Q9<float>& Rr, float gamma, float bn,
+                                               float fbn, float fpsi) {
+    const float tiny = 1e-12f;
+    const float igm1 = 1.0f / (gamma - 1.0f);
+    const float dL = L.v[0], uL = L.v[1], vL = L.v[2], wL = L.v[3], pL = L.v[4], byL = L.v[6], bzL = L.v[7];
+    const float dR = Rr.v[0], uR = Rr.v[1], vR = Rr.v[2], wR = Rr.v[3], pR = Rr.v[4], byR = Rr.v[6], bzR = Rr.v[7];
+    const float bn2 = bn * bn;
+    const float b2L = fmaf(byL, byL, fmaf(bzL, bzL, bn2)), b2R = fmaf(byR, byR, fmaf(bzR, bzR, bn2));
+    const float ptL = fmaf(0.5f, b2L, pL), ptR = fmaf(0.5f, b2R, pR);
+    const float irL = 1.0f / dL, irR = 1.0f / dR;
+    // fast speeds with the common normal field (fast_speed)
+    const float c2L = gamma * pL * irL, c2R = gamma * pR * irR;
+    const float d2L = 0.5f * fmaf(b2L, irL, c2L), d2R = 0.5f * fmaf(b2R, irR, c2R);
+    const float cfL = sqrtf(d2L + sqrtf(fmaxf(fmaf(d2L, d2L, -c2L * bn2 * irL), 0.0f)));
+    const float cfR = sqrtf(d2R + sqrtf(fmaxf(fmaf(d2R, d2R, -c2R * bn2 * irR), 0.0f)));
+    const float EL = fmaf(pL, igm1, fmaf(0.5f * dL, fmaf(uL, uL, fmaf(vL, vL, wL * wL)), 0.5f * b2L));
+    const float ER = fmaf(pR, igm1, fmaf(0.5f * dR, fmaf(uR, uR, fmaf(vR, vR, wR * wR)), 0.5f * b2R));
+    const float cmax = fmaxf(cfL, cfR);
+    const float SL = fminf(fminf(uL, uR) - cmax, 0.0f);
+    const float SR = fmaxf(fmaxf(uL, uR) + cmax, 0.0f);
+    const float aL = (SL - uL) * dL, aR = (SR - uR) * dR;   // rho (S - u) of each side
+    const float iden = 1.0f / (aR - aL);
+    const float SM = (aR * uR - aL * uL - ptR + ptL) * iden;
+    const float pts = (aR * ptL - aL * ptR + aR * aL * (uR - uL)) * iden;
+
+    // the sampled side s (L when SM >= 0) and its star state
+    const bool lside = SM >= 0.0f;
+    const float sig = lside ? -1.0f : 1.0f;   // S*_s = SM + sig |bn| / sqrt(rho*_s)
+    const float d = lside ? dL : dR, u = lside ? uL : uR, v = lside ? vL : vR, w = lside ? wL : wR;
+    const float by = lside ? byL : byR, bz = lside ? bzL : bzR, E = lside ? EL : ER, pt = lside ? ptL : ptR;
+    const float S = lside ? SL : SR, a = lside ? aL : aR;
+    const float isM = 1.0f / (S - SM);
+    const float ds = fmaxf(a * isM, tiny);
+    const float rs = rsqrtf(ds);
+    const float Ss = fmaf(sig * fabsf(bn), rs, SM);
+    float vys, vzs, bys, bzs;
+    {
+        const float denK = a * (S - SM) - bn2;
+        const float ik = 1.0f / denK;
+        const float fac = bn * (SM - u) * ik;
+        const float t = (a * (S - u) - bn2) * ik;
+        const bool degen = fabsf(denK) < tiny;
+        vys = degen ? v : v - by * fac;
+        vzs = degen ? w : w - bz * fac;
+        bys = degen ? by : by * t;
+        bzs = degen ? bz : bz * t;
+    }
+    const float vdotb = u * bn + v * by + w * bz;
+    float vdotbs = SM * bn + vys * bys + vzs * bzs;
+    float Es = ((S - u) * E - pt * u + pts * SM + bn * (vdotb - vdotbs)) * isM;
+    // double-star regions: SL* < 0 <= SM or SM < 0 <= SR*
+    if (lside ? Ss < 0.0f : Ss >= 0.0f) {
+        const float od = lside ? dR : dL, ou = lside ? uR : uL, ov = lside ? vR : vL, ow = lside ? wR : wL;
+        const float oby = lside ? byR : byL, obz = lside ? bzR : bzL, oS = lside ? SR : SL, oa = lside ? aR : aL;
+        const float odsr = fmaxf(oa / (oS - SM), tiny);
+        float ovy, ovz, oby_s, obz_s;
+        {
+            const float denK = oa * (oS - SM) - bn2;
+            const float ik = 1.0f / denK;
+            const float fac = bn * (SM - ou) * ik;
+            const float t = (oa * (oS - ou) - bn2) * ik;
+            const bool degen = fabsf(denK) < tiny;
+            ovy = degen ? ov : ov - oby * fac;
+            ovz = degen ? ow : ow - obz * fac;
+            oby_s = degen ? oby : oby * t;
+            obz_s = degen ? obz : obz * t;
+        }
+        const float sq = ds * rs, osq = sqrtf(odsr);
+        // sgn(bn) times +1 when s = L, -1 when s = R (the averages are antisymmetric in L, R)
+        const float sg = (bn >= 0.0f ? 1.0f : -1.0f) * (lside ? 1.0f : -1.0f);
+        const float invsum = 1.0f / (sq + osq);
+        const float vyss = (sq * vys + osq * ovy + (oby_s - bys) * sg) * invsum;
+        const float vzss = (sq * vzs + osq * ovz + (obz_s - bzs) * sg) * invsum;
+        const float sqq = sq * osq;
+        const float byss = (sq * oby_s + osq * bys + sqq * (ovy - vys) * sg) * invsum;
+        const float bzss = (sq * obz_s + osq * bzs + sqq * (ovz - vzs) * sg) * invsum;
+        const float vdotbss = SM * bn + vyss * byss + vzss * bzss;
+        Es = Es - sq * (vdotbs - vdotbss) * sg;
+        vys = vyss; vzs = vzss; bys = byss; bzs = bzss; vdotbs = vdotbss;
+    }
+    // the physical flux of the sampled state (rho*_s, SM, v, B, E, pT*)
+    const float m = ds * SM;
+    Q9<float> f;
+    f.v[0] = m;
+    f.v[1] = fmaf(m, SM, pts - bn2);
+    f.v[2] = fmaf(m, vys, -bn * bys);
+    f.v[3] = fmaf(m, vzs, -bn * bzs);
+    f.v[4] = fmaf(Es + pts, SM, -bn * vdotbs);
+    f.v[5] = fbn;
+    f.v[6] = fmaf(bys, SM, -bn * vys);
+    f.v[7] = fmaf(bzs, SM, -bn * vzs);
+    f.v[8] = fpsi;
+    return f;
+}
+#endif
+
 template <class R> GMT_HD Q9<R> hlld_x(const Q9<R>& L, const Q9<R>& Rr, R gamma, R bn, R fbn, R fpsi) {
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000) && defined(GMT_PACKED_F32)
+    if constexpr (std::is_same<R, float>::value) return hlld_x_f32(L, Rr, gamma, bn, fbn, fpsi);
+#endif
     const R tiny = R(1e-12);
     R dL = L.v[0], uL = L.v[1], vL = L.v[2], wL = L.v[3], pL = L.v[4], byL = L.v[6], bzL = L.v[7];
     R dR = Rr.v[0], uR = Rr.v[1], vR = Rr.v[2], wR = Rr.v[3], pR = Rr.v[4], byR = Rr.v[6], bzR = Rr.v[7];
