@@ -31,7 +31,8 @@ EXPORTS = (
     "gmt_forcing_reset", "gmt_forcing_advance", "gmt_forcing_set_modes", "gmt_forcing_get_modes",
     "gmt_forcing_counter", "gmt_ic_orszag_tang", "gmt_ic_uniform", "gmt_ic_turbulent", "gmt_ct_step", "gmt_ct_cfl_async",
     "gmt_ct_divb_max", "gmt_ct_ic_orszag_tang", "gmt_ke_spectrum", "gmt_run", "gmt_ensemble_create", "gmt_ensemble_destroy",
-    "gmt_ensemble_run", "gmt_density_pdf", "gmt_ke_band_loss", "gmt_adjoint_step", "gmt_adjoint_amp_grad", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
+    "gmt_ensemble_run", "gmt_density_pdf", "gmt_ke_band_loss", "gmt_adjoint_step", "gmt_adjoint_amp_grad",
+    "gmt_adjoint_set_passes", "gmt_test_wait_limit", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
     "march_set_glm", "march_set_gamma", "march_run_dev", "march_set_nx", "ct_run", "ct_regs", "ct_shmem",
 )
 
@@ -108,6 +109,8 @@ def lib():
             "gmt_density_pdf": ([vp, vp, i32, dbl, dbl, C.POINTER(dbl), C.POINTER(dbl), vp], C.c_int),
             "gmt_adjoint_step": ([vp, vp, vp, vp, A, vp], C.c_int),
             "gmt_adjoint_amp_grad": ([vp, C.POINTER(dbl), i32, vp], C.c_int),
+            "gmt_adjoint_set_passes": ([vp, i32], C.c_int),
+            "gmt_test_wait_limit": ([vp, C.c_int64, i32], C.c_int),
             "gmt_run": ([vp, vp, vp, i32, dbl, dbl, i32, vp, C.POINTER(dbl), C.POINTER(i32)], C.c_int),
             "gmt_ensemble_create": ([P, i32, C.POINTER(i32), C.POINTER(dbl), C.POINTER(C.c_uint32), C.POINTER(vp)],
                                     C.c_int),

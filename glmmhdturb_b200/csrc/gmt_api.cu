@@ -93,6 +93,10 @@ struct gmt_ctx {
     double sigma0 = 0, alpha = 0, beta = 0;
     void* adj = nullptr;           // adjoint scratch (207 planes, allocated on first use)
     double* adj_damp = nullptr;    // dL/d(turb_amp) accumulator
+    int* adj_err = nullptr;        // set when the adjoint's record tile abandons a bounded wait
+    int adj_percell = 0;           // 1: the adjoint runs its first three passes per cell
+    long long wait_cycles = GMT_WAIT_CYCLES;   // budget of the tile kernels' bounded waits
+    int wait_test = 0;             // failure-path tests: staging withheld, so every bounded wait runs out
     struct TmaMap { const void* base; CUtensorMap map; };
     TmaMap tma[2] = {};            // tensor maps of the last two input states (tile staging)
     int tma_next = 0;
@@ -280,6 +284,8 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.trigx = static_cast<const R*>(c->trig[0]);
         A.cfl_out = nullptr;
         A.err = c->err;
+        A.wait_cycles = c->wait_cycles;
+        A.wait_test = c->wait_test;
         A.dx = (R)dx;
         A.dparams = nullptr;
         A.fmass = nullptr;
@@ -310,6 +316,8 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.trigx = static_cast<const R*>(c->trig[0]);
         A.cfl_out = nullptr;
         A.err = c->err;
+        A.wait_cycles = c->wait_cycles;
+        A.wait_test = c->wait_test;
         A.dx = (R)dx;
         A.dparams = nullptr;
         A.fmass = p.nsp > 0 ? static_cast<R*>(c->fmass) : nullptr;
@@ -382,6 +390,8 @@ int ct_step_impl(gmt_ctx* c, const CPlanes8<R>& q, const Planes8<R>& o, const gm
     A.trigx = static_cast<const R*>(c->trig[0]);
     A.scratch = static_cast<R*>(c->ct_scratch);
     A.err = c->err;
+    A.wait_cycles = c->wait_cycles;
+    A.wait_test = c->wait_test;
     set_ct_tma(c, A);
     cudaError_t e = launch_ct(A, s);
     if (e != cudaSuccess) return cuda_fail(e, "ct step");
@@ -546,6 +556,7 @@ int gmt_destroy(gmt_ctx* c) {
     cudaFree(c->spec);
     cudaFree(c->adj);
     cudaFree(c->adj_damp);
+    cudaFree(c->adj_err);
     if (c->cap) cudaStreamDestroy(c->cap);
     cudaFree(c->loop);
     cudaFree(c->loopc);
@@ -745,7 +756,9 @@ int gmt_adjoint_step(gmt_ctx* c, const void* u, const void* ubar_next, void* uba
     if (!c->adj) {
         GMT_CUDA(cudaMalloc(&c->adj, adjoint_scratch_reals(c->n) * c->esize));
         GMT_CUDA(cudaMalloc(&c->adj_damp, sizeof(double)));
+        GMT_CUDA(cudaMalloc(&c->adj_err, sizeof(int)));
         GMT_CUDA(cudaMemsetAsync(c->adj_damp, 0, sizeof(double), s));
+        GMT_CUDA(cudaMemsetAsync(c->adj_err, 0, sizeof(int), s));
     }
     const double dx = p.boxlen / p.nx;
     auto go = [&](auto zero) -> int {
@@ -783,7 +796,9 @@ int gmt_adjoint_step(gmt_ctx* c, const void* u, const void* ubar_next, void* uba
         T.iflo = A.iflo; T.use_llf = A.use_llf; T.do_turb = A.do_turb;
         T.btab = A.btab; T.trigx = A.trigx;
         T.cfl_out = nullptr;
-        T.err = c->err;
+        T.err = c->adj_err;
+        T.wait_cycles = c->wait_cycles;
+        T.wait_test = c->wait_test;
         T.dx = (R)dx;
         T.dparams = nullptr;
         T.fmass = nullptr;
@@ -794,7 +809,7 @@ int gmt_adjoint_step(gmt_ctx* c, const void* u, const void* ubar_next, void* uba
         T.rec_ub = A.ub.p[0];
         T.rec_damp = A.damp;
         T.rec_amp = A.amp;
-        const bool record = c->ox > 0 && c->oy > 0 && c->lz > 0;
+        const bool record = c->ox > 0 && c->oy > 0 && c->lz > 0 && !c->adj_percell;
         cudaError_t e = launch_adjoint<R>(A, record ? &T : nullptr, s);
         return e == cudaSuccess ? GMT_OK : cuda_fail(e, "gmt_adjoint_step");
     };
@@ -805,9 +820,33 @@ int gmt_adjoint_amp_grad(gmt_ctx* c, double* out, int32_t reset, void* stream) {
     if (!c || !out) return fail(GMT_ERR_ARG, "gmt_adjoint_amp_grad: null argument");
     cudaStream_t s = (cudaStream_t)stream;
     if (!c->adj_damp) { *out = 0.0; return GMT_OK; }
+    int herr = 0;
     GMT_CUDA(cudaMemcpyAsync(out, c->adj_damp, sizeof(double), cudaMemcpyDeviceToHost, s));
+    GMT_CUDA(cudaMemcpyAsync(&herr, c->adj_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (reset) GMT_CUDA(cudaMemsetAsync(c->adj_damp, 0, sizeof(double), s));
     GMT_CUDA(cudaStreamSynchronize(s));
+    if (herr) {
+        GMT_CUDA(cudaMemsetAsync(c->adj_err, 0, sizeof(int), s));
+        GMT_CUDA(cudaStreamSynchronize(s));
+        return fail(GMT_ERR_TIMEOUT, "an adjoint step abandoned a bounded wait in its record tile; the gradients "
+                                     "accumulated since the last check are invalid");
+    }
+    return GMT_OK;
+}
+
+int gmt_adjoint_set_passes(gmt_ctx* c, int32_t percell) {
+    if (!c) return fail(GMT_ERR_ARG, "gmt_adjoint_set_passes: null context");
+    c->adj_percell = percell != 0;
+    return GMT_OK;
+}
+
+int gmt_test_wait_limit(gmt_ctx* c, int64_t budget_cycles, int32_t withhold) {
+    if (!c) return fail(GMT_ERR_ARG, "gmt_test_wait_limit: null context");
+    if (budget_cycles < 0) return fail(GMT_ERR_ARG, "gmt_test_wait_limit: budget_cycles must be >= 0");
+    c->wait_cycles = budget_cycles > 0 ? (long long)budget_cycles : GMT_WAIT_CYCLES;
+    c->wait_test = withhold != 0;
+    for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);   // they hold the old kernel arguments
+    c->graphs.clear();
     return GMT_OK;
 }
 
@@ -962,6 +1001,8 @@ cudaError_t run_enqueue(gmt_ctx* c, const void* src, void* dst, int flags, cudaS
     A.trigx = static_cast<const R*>(c->trig[0]);
     A.cfl_out = c->cfl;
     A.err = c->err;
+    A.wait_cycles = c->wait_cycles;
+    A.wait_test = c->wait_test;
     A.dx = (R)(p.boxlen / p.nx);
     A.dparams = reinterpret_cast<const double*>(c->loop);
     A.fmass = nullptr;
@@ -1102,6 +1143,8 @@ template <class R> int ens_bind(gmt_ensemble* E, void* const* u, void* const* w,
             a.trigx = static_cast<const R*>(E->trig[3 * b]);
             a.cfl_out = E->cfl + 2 * b;
             a.err = E->err;
+            a.wait_cycles = GMT_WAIT_CYCLES;
+            a.wait_test = 0;
             a.dx = (R)(E->p.boxlen / n);
             a.dparams = reinterpret_cast<const double*>(E->loop + b);
             a.fmass = nullptr;

@@ -39,6 +39,9 @@ template <class R> struct UnsplitArgs {
                            // for the passive-species pass of the march scheme
     int use_tma;           // tmap describes u: tiles clear of the box edges stage by TMA
     CUtensorMap tmap;      // 4-D map (x, y, z, variable) of u; box (ox+8) x (oy+4) x 1 x 9
+    long long wait_cycles; // budget of each bounded wait (GMT_WAIT_CYCLES)
+    int wait_test;         // failure-path tests only: the next plane is not staged and no thread
+                           // arrives on the staging mbarrier, so every wait runs out (0 in production)
     // adjoint record mode (a scheme with kRecord): the step writes every cell's six interface
     // states and, in place of the new state, the adjoint of its update epilogue
     R* rec_fs;             // 54 planes: interface states +x, -x, +y, -y, +z, -z of every cell
@@ -130,12 +133,22 @@ __device__ __forceinline__ void tma_load_4d(void* smem_dst, const CUtensorMap* m
         : "memory");
 }
 
-// bounded wait: gives up after ~2^20 polls, records the failure and returns false
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err) {
-    for (int it = 0; it < (1 << 20); ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    if (err) atomicExch(err, 1);
-    return false;
+// Bounded wait for an mbarrier phase: polls until the phase completes or `budget` SM clock
+// cycles (clock64) have passed since the first poll; then it records the failure in *err and
+// returns false, and the caller carries on (its output is reported invalid by the host).
+// GMT_WAIT_CYCLES, about 0.5 s at the B200's 1.965 GHz, is the default budget of the tile kernels;
+// a staged plane lands in microseconds.
+#define GMT_WAIT_CYCLES (1LL << 30)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err, long long budget) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > budget) {
+            if (err) atomicExch(err, 1);
+            return false;
+        }
+    }
+    return true;
 }
 
 template <class R> __device__ __forceinline__ void cp_async_r(R* smem, const R* gmem);

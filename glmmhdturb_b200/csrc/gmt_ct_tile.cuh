@@ -197,7 +197,7 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
     // one copy of the 8 state variables of plane k+2 and one of bzf at k+3 per plane
     bool tma = false;
     {
-        tma = A.use_tma && x0 >= 4 && x0 + OX + 4 <= nx && y0 >= 2 && y0 + OY + 3 <= ny;
+        tma = A.use_tma && !A.wait_test && x0 >= 4 && x0 + OX + 4 <= nx && y0 >= 2 && y0 + OY + 3 <= ny;
         if ((unsigned)__cvta_generic_to_shared(SG) & 127u) tma = false;
     }
     const unsigned tma_bytes = (unsigned)(9 * SN5 * sizeof(R));
@@ -240,7 +240,7 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
                     tma_load_4d(SG + 8 * SN5, &A.tmap1, x0 - 4, y0 - 2, wrapi(kr + 3, nz), 7, mbar);
                 }
             }
-            if (!tma) {
+            if (!tma && !A.wait_test) {
                 ct_stage_plane(SG, A.q, PN5, PW5, SW, SN5, x0, y0, kr + 2, nx, ny, nz, tid >= stg0 ? tid - stg0 : PN5,
                                NT - stg0);
                 mbar_arrive_cp_async(mbar);
@@ -357,7 +357,7 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
             }
         }
         if (load) {
-            mbar_wait(mbar, phase, A.err);
+            mbar_wait(mbar, phase, A.err, A.wait_cycles);
             phase ^= 1u;
             ct_unstage_plane(PR + mod3(kr + 2) * 9 * PN, FB + mod3(kr + 2) * 3 * PN, SG, PN, PW, SN5, SW, K,
                              tid < nunst ? tid : PN, nunst);

@@ -64,6 +64,8 @@ template <class R> struct CTArgs {
     int use_tma;           // tmap8/tmap1 describe q: tiles clear of the box edges stage by TMA
     CUtensorMap tmap8;     // 4-D map (x, y, z, variable) of q, box (ox+8) x (oy+5) x 1 x 8
     CUtensorMap tmap1;     // the same tensor, box (ox+8) x (oy+5) x 1 x 1 (bzf of the next plane)
+    long long wait_cycles; // budget of each bounded wait (GMT_WAIT_CYCLES)
+    int wait_test;         // failure-path tests only (see UnsplitArgs::wait_test)
 };
 cudaError_t launch_ct(const CTArgs<float>& A, cudaStream_t s);
 cudaError_t launch_ct(const CTArgs<double>& A, cudaStream_t s);

@@ -2,9 +2,10 @@
 // HLLD|HLL|LLF + Dedner GLM + void floor + psi damping + mode-sum forcing kick (+ next-step CFL).
 //
 // Layout.  A block owns an OX x OY column tile of the periodic box over a chunk of LZ planes and
-// marches z.  Shared memory holds
-//   PR[3][9][(OX+4)(OY+4)]  primitive ring (planes k-1, k, k+1; 2-cell in-plane halo),
-//   ST[4][9][(OX+2)(OY+2)]  in-plane interface states +x,-x,+y,-y of the reconstruction region,
+// marches z.  Shared memory holds (9-variable arrays in the Lay layout below: FP32 cells as two
+// 16-byte vectors and a scalar)
+//   PR[3][(OX+4)(OY+4)]     primitive ring (planes k-1, k, k+1; 2-cell in-plane halo),
+//   ST[4][(OX+2)(OY+2)]     in-plane interface states +x,-x,+y,-y of the reconstruction region,
 //                           overwritten in place by the face fluxes,
 //   SG[9][(OY+4)][OX+8]     conserved staging plane k+2 (the ring region at column offset 2),
 //                           filled while plane k computes.
@@ -28,6 +29,41 @@ template <class R> struct Rec {
     bool up;
 };
 
+// Shared-memory layout of the 9-variable arrays (the primitive ring, the interface states): an
+// array of n cells, padded to lay_n(n) cells.  FP32: per cell the variables 0-3 and 4-7 as two
+// 16-byte vectors and variable 8 alone ([A: float4 x n][B: float4 x n][C: float x n]), so one
+// cell's 9 values take two 128-bit and one 32-bit access (a warp's 32 consecutive cells read
+// 512 contiguous bytes per vector, conflict-free).  FP64: 9 scalar planes ([v][n]).
+template <class R> __host__ __device__ constexpr int lay_n(int n) { return sizeof(R) == 4 ? (n + 3) & ~3 : n; }
+template <class R> struct Lay {
+    static __device__ __forceinline__ Q9<R> get(const R* __restrict__ S, int n, int c) {
+        Q9<R> q;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) q.v[v] = S[v * n + c];
+        return q;
+    }
+    static __device__ __forceinline__ void put(R* __restrict__ S, int n, int c, const Q9<R>& q) {
+#pragma unroll
+        for (int v = 0; v < 9; ++v) S[v * n + c] = q.v[v];
+    }
+    static __device__ __forceinline__ R get1(const R* __restrict__ S, int n, int c, int v) { return S[v * n + c]; }
+};
+template <> struct Lay<float> {
+    static __device__ __forceinline__ Q9<float> get(const float* __restrict__ S, int n, int c) {
+        const float4 a = reinterpret_cast<const float4*>(S)[c];
+        const float4 b = reinterpret_cast<const float4*>(S)[n + c];
+        return Q9<float>{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, S[8 * n + c]}};
+    }
+    static __device__ __forceinline__ void put(float* __restrict__ S, int n, int c, const Q9<float>& q) {
+        reinterpret_cast<float4*>(S)[c] = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
+        reinterpret_cast<float4*>(S)[n + c] = make_float4(q.v[4], q.v[5], q.v[6], q.v[7]);
+        S[8 * n + c] = q.v[8];
+    }
+    static __device__ __forceinline__ float get1(const float* __restrict__ S, int n, int c, int v) {
+        return v < 8 ? S[4 * (v < 4 ? c : n + c) + (v & 3)] : S[8 * n + c];
+    }
+};
+
 template <class R, int RECON>
 __device__ __forceinline__ void recon_prims(const R* __restrict__ PR, int PN, int PW, int c, int s0, int sm, int sp,
                                             const Consts<R>& K, R dtdx, Rec<R>& r) {
@@ -37,18 +73,17 @@ __device__ __forceinline__ void recon_prims(const R* __restrict__ PR, int PN, in
     Q9<R> L, Rr;
     constexpr bool MM = RECON == RECON_MINMOD;
     bool up = true;
-#pragma unroll
-    for (int v = 0; v < 9; ++v) r.m0.v[v] = P0[v * PN + c];
-#pragma unroll
-    for (int v = 0; v < 9; ++v) { L.v[v] = P0[v * PN + c - 1]; Rr.v[v] = P0[v * PN + c + 1]; }
+    r.m0 = Lay<R>::get(P0, PN, c);
+    L = Lay<R>::get(P0, PN, c - 1);
+    Rr = Lay<R>::get(P0, PN, c + 1);
     r.s[0] = half_slope<MM>(L, r.m0, Rr);
     if (RECON == RECON_PPM) up = up && !spj(L.v[4], r.m0.v[4], Rr.v[4]);
-#pragma unroll
-    for (int v = 0; v < 9; ++v) { L.v[v] = P0[v * PN + c - PW]; Rr.v[v] = P0[v * PN + c + PW]; }
+    L = Lay<R>::get(P0, PN, c - PW);
+    Rr = Lay<R>::get(P0, PN, c + PW);
     r.s[1] = half_slope<MM>(L, r.m0, Rr);
     if (RECON == RECON_PPM) up = up && !spj(L.v[4], r.m0.v[4], Rr.v[4]);
-#pragma unroll
-    for (int v = 0; v < 9; ++v) { L.v[v] = Pm[v * PN + c]; Rr.v[v] = Pp[v * PN + c]; }
+    L = Lay<R>::get(Pm, PN, c);
+    Rr = Lay<R>::get(Pp, PN, c);
     r.s[2] = half_slope<MM>(L, r.m0, Rr);
     if (RECON == RECON_PPM) up = up && !spj(L.v[4], r.m0.v[4], Rr.v[4]);
     r.up = up;
@@ -68,10 +103,11 @@ __device__ __forceinline__ Q9<R> face_state(const Rec<R>& r, const R* __restrict
         if (D == 0) { PL = PRr = PR + (size_t)s0 * 9 * PN; cl = c - 1; cr = c + 1; }
         else if (D == 1) { PL = PRr = PR + (size_t)s0 * 9 * PN; cl = c - PW; cr = c + PW; }
         else { PL = PR + (size_t)sm * 9 * PN; PRr = PR + (size_t)sp * 9 * PN; cl = c; cr = c; }
+        const Q9<R> qm = Lay<R>::get(PL, PN, cl), qp = Lay<R>::get(PRr, PN, cr);
 #pragma unroll
         for (int v = 0; v < 9; ++v) {
             R lo, hi;
-            ppm_edges(PL[v * PN + cl], r.m0.v[v], PRr[v * PN + cr], lo, hi);
+            ppm_edges(qm.v[v], r.m0.v[v], qp.v[v], lo, hi);
             f.v[v] = r.mh.v[v] + (SIGN > 0 ? hi : lo) - r.m0.v[v];
         }
     } else {
@@ -84,6 +120,7 @@ __device__ __forceinline__ Q9<R> face_state(const Rec<R>& r, const R* __restrict
     return f;
 }
 
+// 9 scalar planes of RN cells (the CT tile's state arrays)
 template <class R> __device__ __forceinline__ void st_put(R* __restrict__ S, int RN, int idx, const Q9<R>& q) {
 #pragma unroll
     for (int v = 0; v < 9; ++v) S[v * RN + idx] = q.v[v];
@@ -118,24 +155,24 @@ __device__ __forceinline__ void stage_plane(R* __restrict__ SG, const CPlanes<R>
     cp_async_commit();
 }
 
+// PN: the ring's padded array length (the layout stride); PNc: the ring cells to convert
 template <class R>
-__device__ __forceinline__ void unstage_plane(R* __restrict__ PRs, const R* __restrict__ SG, int PN, int PW, int SW,
-                                              int SN, const Consts<R>& K, R pfloor, int tid, int nt) {
-    for (int c = tid; c < PN; c += nt) {
+__device__ __forceinline__ void unstage_plane(R* __restrict__ PRs, const R* __restrict__ SG, int PN, int PNc, int PW,
+                                              int SW, int SN, const Consts<R>& K, R pfloor, int tid, int nt) {
+    for (int c = tid; c < PNc; c += nt) {
         const int cs = (c / PW) * SW + c % PW + 2;
         Q9<R> q;
 #pragma unroll
         for (int v = 0; v < 9; ++v) q.v[v] = SG[v * SN + cs];
         q = cons2prim(q, K.gamma, K.smallr, pfloor);
-#pragma unroll
-        for (int v = 0; v < 9; ++v) PRs[v * PN + c] = q.v[v];
+        Lay<R>::put(PRs, PN, c, q);
     }
 }
 
 // shared-memory layout of the tile march: PR ring, ST states, then (128-byte aligned, as a TMA
 // destination) the staging plane SG, then (16-byte aligned) the reduction and mbarrier words
 template <class R> __host__ __device__ inline size_t unsplit_sg_offset(int ox, int oy) {
-    size_t PN = (size_t)(ox + 4) * (oy + 4), RN = (size_t)(ox + 2) * (oy + 2);
+    size_t PN = (size_t)lay_n<R>((ox + 4) * (oy + 4)), RN = (size_t)lay_n<R>((ox + 2) * (oy + 2));
     return ((27 * PN + 36 * RN) * sizeof(R) + 127) / 128 * 128;
 }
 template <class R> __host__ __device__ inline size_t unsplit_red_offset(int ox, int oy) {
@@ -199,9 +236,7 @@ template <class R, int RECON> struct MarchScheme {
     static __device__ __forceinline__ R prim_floor(const Consts<R>& K) { return K.smallp; }
     static __device__ __forceinline__ void recon(const R* PR, int PN, int, int c, int s0, int, int, const Consts<R>&, R,
                                                  Cell& r) {
-        const R* P0 = PR + (size_t)s0 * 9 * PN;
-#pragma unroll
-        for (int v = 0; v < 9; ++v) r.m0.v[v] = P0[v * PN + c];
+        r.m0 = Lay<R>::get(PR + (size_t)s0 * 9 * PN, PN, c);
     }
     template <int D>
     static __device__ __forceinline__ void neighbours(const R* PR, int PN, int PW, int c, int s0, int sm, int sp,
@@ -209,8 +244,8 @@ template <class R, int RECON> struct MarchScheme {
         const R* PL = PR + (size_t)(D == 2 ? sm : s0) * 9 * PN;
         const R* PP = PR + (size_t)(D == 2 ? sp : s0) * 9 * PN;
         const int cl = D == 0 ? c - 1 : (D == 1 ? c - PW : c), cr = D == 0 ? c + 1 : (D == 1 ? c + PW : c);
-#pragma unroll
-        for (int v = 0; v < 9; ++v) { L.v[v] = PL[v * PN + cl]; Rr.v[v] = PP[v * PN + cr]; }
+        L = Lay<R>::get(PL, PN, cl);
+        Rr = Lay<R>::get(PP, PN, cr);
     }
     template <int D>
     static __device__ __forceinline__ void prep(Cell& r, const R* PR, int PN, int PW, int c, int s0, int sm, int sp,
@@ -263,8 +298,9 @@ template <class R, class S, int TOX, int TOY, bool OVERHANG = false, bool TMA = 
 __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepVals<R>& V, int bx, int by, int bz,
                                             unsigned char* smem_raw) {
     const int OX = TOX > 0 ? TOX : A.ox, OY = TOY > 0 ? TOY : A.oy;
-    const int PW = OX + 4, PN = (OX + 4) * (OY + 4);
-    const int RW = OX + 2, RN = (OX + 2) * (OY + 2);
+    const int PW = OX + 4, PN = lay_n<R>((OX + 4) * (OY + 4));     // padded array lengths
+    const int RW = OX + 2, RN = lay_n<R>((OX + 2) * (OY + 2));
+    const int PNc = (OX + 4) * (OY + 4);                             // ring cells per plane
     const int SW = OX + 8, SN = (OX + 8) * (OY + 4);
     R* PR = reinterpret_cast<R*>(smem_raw);
     R* ST = PR + 27 * PN;
@@ -293,7 +329,7 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     // every tile when the caller supplied no map, by per-thread cp.async
     bool tma = false;
     if constexpr (TMA) {
-        tma = A.use_tma && x0 >= 4 && x0 + OX + 4 <= nx && y0 >= 2 && y0 + OY + 2 <= ny;
+        tma = A.use_tma && !A.wait_test && x0 >= 4 && x0 + OX + 4 <= nx && y0 >= 2 && y0 + OY + 2 <= ny;
         // a TMA destination must be 128-byte aligned; otherwise stay on cp.async
         if ((unsigned)__cvta_generic_to_shared(SG) & 127u) tma = false;
     }
@@ -302,10 +338,10 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     // prologue: primitives of planes z0-2, z0-1, z0
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
     for (int j = 0; j < 3; ++j) {
-        stage_plane(SG, A.u, PN, PW, SW, SN, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
+        stage_plane(SG, A.u, PNc, PW, SW, SN, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
         cp_async_wait_all();
         __syncthreads();
-        unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, SG, PN, PW, SW, SN, K, S::prim_floor(K), tid, NT);
+        unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, SG, PN, PNc, PW, SW, SN, K, S::prim_floor(K), tid, NT);
         if (j == 2 && tid == 0) {
             mbar_init(mbar, tma ? 1u : (unsigned)NT);
             if (tma) fence_mbar_init();
@@ -352,8 +388,8 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
                     }
                 }
             }
-            if (!tma) {
-                stage_plane(SG, A.u, PN, PW, SW, SN, x0, y0, kr + 2, nx, ny, nz, tid >= stg0 ? tid - stg0 : PN,
+            if (!tma && !A.wait_test) {
+                stage_plane(SG, A.u, PNc, PW, SW, SN, x0, y0, kr + 2, nx, ny, nz, tid >= stg0 ? tid - stg0 : PNc,
                             NT - stg0);
                 mbar_arrive_cp_async(mbar);
             }
@@ -362,53 +398,55 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
             Q9<R> XY;
             R fmx = R(0), fmy = R(0);   // lower-face mass fluxes, kept when A.fmass is set
             if (kr - 1 >= z0) {
+                const Q9<R> Fxl = Lay<R>::get(ST + 1 * 9 * RN, RN, rown), Fyl = Lay<R>::get(ST + 3 * 9 * RN, RN, rown);
 #pragma unroll
-                for (int v = 0; v < 9; ++v)
-                    XY.v[v] = (ST[(1 * 9 + v) * RN + rown] - Fxh.v[v]) + (ST[(3 * 9 + v) * RN + rown] - Fyh.v[v]);
+                for (int v = 0; v < 9; ++v) XY.v[v] = (Fxl.v[v] - Fxh.v[v]) + (Fyl.v[v] - Fyh.v[v]);
                 if (A.fmass) {
-                    fmx = ST[(1 * 9 + 0) * RN + rown];
-                    fmy = ST[(3 * 9 + 0) * RN + rown];
+                    fmx = Fxl.v[0];
+                    fmy = Fyl.v[0];
                 }
             }
             typename S::Cell r;
             S::recon(PR, PN, PW, cown, s0, sm, sp, K, dtdx, r);
-            // the own cell of plane kr (a cell of this chunk when kr is neither first nor last)
-            const size_t gk = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * (size_t)(kr < 0 ? 0 : kr));
+            // record mode: interface state k of the own cell of plane kr, written only for a plane of
+            // this chunk (z0 <= kr < z1)
             const size_t ncell = (size_t)nx * ny * nz;
+            auto record = [&](int k, const Q9<R>& f) {
+                if constexpr (S::kRecord) {
+                    if (kr >= z0 && kr < z1)
+                        rec_put(A, ncell, k, (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * (size_t)kr), f);
+                }
+            };
             if (!first && !last) {
                 S::template prep<0>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx);
                 {
                     const Q9<R> f = S::template state<0, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
-                    st_put(ST + 0 * 9 * RN, RN, rown, f);
-                    if constexpr (S::kRecord) rec_put(A, ncell, 0, gk, f);
+                    Lay<R>::put(ST + 0 * 9 * RN, RN, rown, f);
+                    record(0, f);
                 }
                 {
                     const Q9<R> f = S::template state<0, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
-                    st_put(ST + 1 * 9 * RN, RN, rown, f);
-                    if constexpr (S::kRecord) rec_put(A, ncell, 1, gk, f);
+                    Lay<R>::put(ST + 1 * 9 * RN, RN, rown, f);
+                    record(1, f);
                 }
                 S::template prep<1>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx);
                 {
                     const Q9<R> f = S::template state<1, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
-                    st_put(ST + 2 * 9 * RN, RN, rown, f);
-                    if constexpr (S::kRecord) rec_put(A, ncell, 2, gk, f);
+                    Lay<R>::put(ST + 2 * 9 * RN, RN, rown, f);
+                    record(2, f);
                 }
                 {
                     const Q9<R> f = S::template state<1, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
-                    st_put(ST + 3 * 9 * RN, RN, rown, f);
-                    if constexpr (S::kRecord) rec_put(A, ncell, 3, gk, f);
+                    Lay<R>::put(ST + 3 * 9 * RN, RN, rown, f);
+                    record(3, f);
                 }
             }
             S::template prep<2>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx);
             Q9<R> Pz = S::template state<2, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
-            if constexpr (S::kRecord) {
-                if (!first && !last) rec_put(A, ncell, 4, gk, Pz);
-            }
+            if (!first && !last) record(4, Pz);
             if (!first) {
                 Q9<R> Mz = S::template state<2, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
-                if constexpr (S::kRecord) {
-                    if (!last) rec_put(A, ncell, 5, gk, Mz);
-                }
+                if (!last) record(5, Mz);
                 Q9<R> Fzhi = S::template flux<2>(pPz, Mz, K, ch, A.use_llf != 0);
                 if (kr - 1 >= z0) {
                     const int kf = kr - 1;
@@ -474,39 +512,39 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
                     if (which == 2) f = S::template state<1, +1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
                     else f = S::template state<1, -1>(r, PR, PN, PW, cc, s0, sm, sp, K, A.iflo);
                 }
-                st_put(ST + which * 9 * RN, RN, rc, f);
+                Lay<R>::put(ST + which * 9 * RN, RN, rc, f);
             }
         }
         __syncthreads();
         if (!first && !last) {
             // own faces at x+1/2 and y+1/2: flux kept in registers and written over the right state,
             // where the neighbour reads it as its lower-face flux
-            Fxh = S::template flux<0>(st_get(ST + 0 * 9 * RN, RN, rown), st_get(ST + 1 * 9 * RN, RN, ixh), K, ch,
+            Fxh = S::template flux<0>(Lay<R>::get(ST + 0 * 9 * RN, RN, rown), Lay<R>::get(ST + 1 * 9 * RN, RN, ixh), K, ch,
                                       A.use_llf != 0);
-            st_put(ST + 1 * 9 * RN, RN, ixh, Fxh);
-            Fyh = S::template flux<1>(st_get(ST + 2 * 9 * RN, RN, rown), st_get(ST + 3 * 9 * RN, RN, iyh), K, ch,
+            Lay<R>::put(ST + 1 * 9 * RN, RN, ixh, Fxh);
+            Fyh = S::template flux<1>(Lay<R>::get(ST + 2 * 9 * RN, RN, rown), Lay<R>::get(ST + 3 * 9 * RN, RN, iyh), K, ch,
                                       A.use_llf != 0);
-            st_put(ST + 3 * 9 * RN, RN, iyh, Fyh);
+            Lay<R>::put(ST + 3 * 9 * RN, RN, iyh, Fyh);
             for (int h = NT - 1 - tid; h < OX + OY; h += NT) {
                 // boundary faces on the low x and low y side of the tile, taken by the last threads
                 if (h < OY) {
                     const int il = 0 + RW * (h + 1), ir = 1 + RW * (h + 1);
-                    Q9<R> F = S::template flux<0>(st_get(ST + 0 * 9 * RN, RN, il), st_get(ST + 1 * 9 * RN, RN, ir), K,
+                    Q9<R> F = S::template flux<0>(Lay<R>::get(ST + 0 * 9 * RN, RN, il), Lay<R>::get(ST + 1 * 9 * RN, RN, ir), K,
                                                   ch, A.use_llf != 0);
-                    st_put(ST + 1 * 9 * RN, RN, ir, F);
+                    Lay<R>::put(ST + 1 * 9 * RN, RN, ir, F);
                 } else {
                     const int c = h - OY;
                     const int il = (c + 1), ir = (c + 1) + RW;
-                    Q9<R> F = S::template flux<1>(st_get(ST + 2 * 9 * RN, RN, il), st_get(ST + 3 * 9 * RN, RN, ir), K,
+                    Q9<R> F = S::template flux<1>(Lay<R>::get(ST + 2 * 9 * RN, RN, il), Lay<R>::get(ST + 3 * 9 * RN, RN, ir), K,
                                                   ch, A.use_llf != 0);
-                    st_put(ST + 3 * 9 * RN, RN, ir, F);
+                    Lay<R>::put(ST + 3 * 9 * RN, RN, ir, F);
                 }
             }
         }
         if (load) {
-            mbar_wait(mbar, phase, A.err);
+            mbar_wait(mbar, phase, A.err, A.wait_cycles);
             phase ^= 1u;
-            unstage_plane(PR + mod3(kr + 2) * 9 * PN, SG, PN, PW, SW, SN, K, S::prim_floor(K), tid < nunst ? tid : PN,
+            unstage_plane(PR + mod3(kr + 2) * 9 * PN, SG, PN, PNc, PW, SW, SN, K, S::prim_floor(K), tid < nunst ? tid : PNc,
                           nunst);
         }
         __syncthreads();

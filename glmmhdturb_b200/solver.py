@@ -197,6 +197,17 @@ class Solver:
         check(lib().gmt_adjoint_step(self._ctx, self._ptr(u), self._ptr(ubar_next), self._ptr(ubar), C.byref(a),
                                      _stream_handle(stream)))
 
+    def adjoint_set_passes(self, percell: bool):
+        """percell=True: the FP32 adjoint runs its first three passes per cell instead of as the
+        record-mode tile march (the check of the tile form; gmt_adjoint_set_passes)."""
+        check(lib().gmt_adjoint_set_passes(self._ctx, int(bool(percell))))
+
+    def test_wait_limit(self, budget_cycles=0, withhold=False):
+        """Failure-path tests only: bounded-wait budget in SM cycles, and withhold=True to skip the
+        staging of each next plane so every wait runs out (gmt_test_wait_limit); (0, False)
+        restores production behaviour."""
+        check(lib().gmt_test_wait_limit(self._ctx, int(budget_cycles), int(bool(withhold))))
+
     def adjoint_amp_grad(self, reset=True, stream=None) -> float:
         out = C.c_double()
         check(lib().gmt_adjoint_amp_grad(self._ctx, C.byref(out), int(bool(reset)), _stream_handle(stream)))

@@ -178,8 +178,15 @@ int gmt_ke_band_loss(gmt_ctx* ctx, const void* u, int32_t kmin, int32_t kmax, do
  * ubar must not alias u or ubar_next.  PPM and non-unsplit contexts return GMT_ERR_ARG. */
 int gmt_adjoint_step(gmt_ctx* ctx, const void* u, const void* ubar_next, void* ubar, const gmt_step_args* a,
                      void* stream);
-/* *out = the accumulated dL/d(turb_amp); reset != 0 zeroes the accumulator afterwards.  Synchronous. */
+/* *out = the accumulated dL/d(turb_amp); reset != 0 zeroes the accumulator afterwards.  Synchronous.
+ * Returns GMT_ERR_TIMEOUT (and clears the condition) if an adjoint step since the last call abandoned
+ * a bounded wait: the gradients accumulated since then are invalid. */
 int gmt_adjoint_amp_grad(gmt_ctx* ctx, double* out, int32_t reset, void* stream);
+/* The FP32 adjoint runs its first three passes (interface states, fluxes, update-epilogue adjoint)
+ * as the forward step's tile march in record mode; percell != 0 makes it run them as per-cell passes
+ * instead (the FP64 path always does).  Both give the same gradient to round-off; the per-cell form
+ * is the check of the tile form.  No counterpart in the reference. */
+int gmt_adjoint_set_passes(gmt_ctx* ctx, int32_t percell);
 
 /* --- diagnostics without allocation --------------------------------------------------------
  * No counterpart in the reference.  Same quantities as gmt_diagnostics for a 9-plane GLM state,
@@ -193,6 +200,16 @@ int gmt_adjoint_amp_grad(gmt_ctx* ctx, double* out, int32_t reset, void* stream)
 #define GMT_NOALLOC_MAX_PLANES 2048
 int gmt_diagnostics_noalloc(const void* u, int32_t nx, int32_t ny, int32_t nz, int32_t dtype, double boxlen,
                             double smallr, gmt_diag* out, void* stream);
+
+/* --- failure-path testing (no counterpart in the reference) ------------------------------------
+ * The tile kernels (GLM, march, CT, the adjoint's record tile) wait for each staged plane on an
+ * mbarrier with a bounded wait: after budget_cycles SM clock cycles (default 2^30, about 0.5 s) a
+ * wait gives up, sets the context's error flag and the kernel finishes; the host then reports
+ * GMT_ERR_TIMEOUT (gmt_cfl_result, gmt_run, gmt_adjoint_amp_grad) and the step's output is invalid.
+ * This sets the budget (budget_cycles = 0: the default) and, with withhold != 0, makes the tiles
+ * skip staging the next plane and withhold their arrivals, so that every wait runs out with no
+ * copy in flight.  (0, 0) restores production behaviour.  For tests of the failure path only. */
+int gmt_test_wait_limit(gmt_ctx* ctx, int64_t budget_cycles, int32_t withhold);
 
 /* --- forcing: 61 +/- integer modes, 1 <= |k|^2 <= 9, solenoidal OU, Philox4x32-10 -------- */
 int gmt_forcing_reset(gmt_ctx* ctx, void* stream);
