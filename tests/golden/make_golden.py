@@ -65,6 +65,13 @@ def ct_state(seed=0):
     return q
 
 
+def calibrated_amp():
+    """The forcing amplitude of the 64^3 parity configuration (amp_calibration.json, written by
+    calibrate_amp.py: rms Mach 1 at t = 2 tau with the FP64 oracle)."""
+    import json
+    return float(json.load(open(os.path.join(HERE, "amp_calibration.json")))["amp"])
+
+
 def forcing_modes():
     f = O.OUForcing(amp=3.0, T=0.5, ndt=100, seed=0)
     for _ in range(3):

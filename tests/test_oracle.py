@@ -253,3 +253,15 @@ def test_branch_counts_zero_on_a_smooth_state(oracle, golden):
     for k in ("hancock_revert", "iflo_revert", "void_floor", "llf_switch", "hlld_degen"):
         assert bc.counts[k] == 0, (k, bc.counts)
     assert sum(bc.counts[k] for k in ("hlld_L", "hlld_Ls", "hlld_Rs", "hlld_R")) >= 3 * 512
+
+
+def test_calibrated_amplitude_is_used_everywhere():
+    """The configs' forcing amplitude comes from the committed calibration (rms Mach 1 at t = 2 tau,
+    FP64 oracle at 64^3, tests/golden/calibrate_amp.py) and the bench uses the same number."""
+    import json
+    import os
+    cal = json.load(open(os.path.join(os.path.dirname(G.__file__), "amp_calibration.json")))
+    assert abs(cal["mach_at_t_cal"] - 1.0) <= cal["tol"]
+    assert G.calibrated_amp() == cal["amp"]
+    import bench
+    assert bench.AMP == cal["amp"]
