@@ -4,8 +4,10 @@
 Workload (one "step" = one full time step of the 512^3 periodic box, FP32): CFL reduction fused
 into the previous step's write-out, host dt/ch from it (as compute_dt does), OU mode forcing update
 on the reference cadence, and the fused unsplit PLM(MC) + MUSCL-Hancock + HLLD + Dedner GLM step
-with the forcing kick.  Initial state: seeded synthetic turbulence (rms Mach 1, gamma 5/3, rho 1,
-p 0.6, B0 = (0.775, 0, 0)) standing in for the pre-evolved checkpoint of the 512^3 configuration.
+with the forcing kick.  Initial state: the pre-evolved turbulent state of the 512^3 configuration,
+made outside the timed region by a forced spin-up with seed 1 from the uniform state (gamma 5/3,
+rho 1, p 0.6, B0 = (0.775, 0, 0)) to rms Mach 1 (checkpoint.spinup_levels: 64^3 until Mach 0.95,
+then 128^3 and 256^3, then 512^3 until Mach 1); the timed steps continue its forcing.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--scheme unsplit|ct|march1d] [--n N] [--dtype f32|f64] [--recon mc|ppm] [--riemann hlld|hll]
@@ -30,7 +32,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_DEFAULT = 512
-AMP = 2.0            # forcing amplitude (stationary rms acceleration)
+AMP = 3.7737         # forcing amplitude (stationary rms acceleration): rms Mach 1 at t = 2 tau from the
+                     # uniform state (tests/golden/amp_calibration.json, by tests/golden/calibrate_amp.py)
 COURANT = 0.3
 CP_COEF = 0.18
 GAMMA = 5.0 / 3.0
@@ -59,6 +62,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--tile", default="", help="force tile as X,Y,Z")
+    ap.add_argument("--ic", default="spinup", choices=["spinup", "synthetic"],
+                    help="forced spin-up to rms Mach 1 (unsplit, march1d) or seeded synthetic turbulence")
     a = ap.parse_args()
     if a.riemann is None:
         a.riemann = "hll" if a.scheme == "march1d" else "hlld"
@@ -314,15 +319,31 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     u = s.alloc()
     w = s.alloc()
-    s.ic_turbulent(u, 1.0, 0.6, (0.775, 0.0, 0.0), mach=1.0, db=0.1, seed=1)
+    ic_note = "seeded synthetic turbulence, Mach 1, seed 1"
+    if args.ic == "spinup" and args.scheme != "ct" and n % 64 == 0 and n & (n - 1) == 0:
+        from glmmhdturb_b200 import checkpoint
+        us, t_spin, levels, ss = checkpoint.spinup_levels(n, seed=1, amp=AMP, mach_target=1.0, dtype=args.dtype,
+                                                          gamma=GAMMA, courant=COURANT, tile=tile)
+        u.copy_(us)
+        fstate0 = ss.forcing_state()
+        del us, ss
+        torch.cuda.empty_cache()
+        ic_note = (f"forced spin-up from the uniform state, seed 1, amp {AMP}, to rms Mach {levels[-1][3]:.3f} at "
+                   f"t = {t_spin:.4f}: " + ", ".join(f"{m}^3 to t = {te:.4f} ({k} steps, Mach {mc:.3f})"
+                                                      for m, te, k, mc in levels))
+    else:
+        s.ic_turbulent(u, 1.0, 0.6, (0.775, 0.0, 0.0), mach=1.0, db=0.1, seed=1)
+        s.forcing_reset()
+        s.forcing_advance()
+        fstate0, t_spin = s.forcing_state(), 0.0
+    u0 = u.clone()
     zones = s.n
     state_bytes = u.numel() * u.element_size()
     st = {"t": 0.0, "launches": 0}
 
     def begin():
-        s.forcing_reset()
-        s.forcing_advance()
-        st["t"] = 0.0
+        s.set_forcing_state(fstate0)
+        st["t"] = t_spin
         st["cm"], st["sm"] = s.cfl(u)
 
     kernel_events = []
@@ -383,8 +404,8 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         host_in = torch.empty(u.shape, dtype=u.dtype, pin_memory=True)
-        s.ic_turbulent(w, 1.0, 0.6, (0.775, 0.0, 0.0), mach=1.0, db=0.1, seed=1)
-        host_in.copy_(w)
+        host_in.copy_(u0)
+        del u0
         host_out = torch.empty_like(host_in, pin_memory=True)
         torch.cuda.synchronize()
         barrier()
@@ -422,7 +443,8 @@ def run_ours(args):
                "vs_baseline": value / PUBLISHED_A6000 if args.scheme == "unsplit" and args.n == 512 else None,
                "dtype": args.dtype,
                "data": "synthetic",
-               "config": workload_config(args, {"parallelism": f"replicas{world}" if world > 1 else "single",
+               "config": workload_config(args, {"ic": ic_note,
+                                                "parallelism": f"replicas{world}" if world > 1 else "single",
                                                 "tile": list(info["tile"]), "regs": info["regs"],
                                                 "smem_bytes": info["smem"], "autotune": tuned}),
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -29,7 +29,7 @@ EXPORTS = (
     "gmt_version", "gmt_last_error", "gmt_params_init", "gmt_create", "gmt_destroy", "gmt_kernel_info",
     "gmt_step", "gmt_step_planes", "gmt_cfl_async", "gmt_cfl_result", "gmt_compute_dt", "gmt_diagnostics", "gmt_diagnostics_noalloc",
     "gmt_forcing_reset", "gmt_forcing_advance", "gmt_forcing_set_modes", "gmt_forcing_get_modes",
-    "gmt_forcing_counter", "gmt_ic_orszag_tang", "gmt_ic_uniform", "gmt_ic_turbulent", "gmt_ct_step", "gmt_ct_cfl_async",
+    "gmt_forcing_counter", "gmt_forcing_get_state", "gmt_forcing_set_state", "gmt_ic_orszag_tang", "gmt_ic_uniform", "gmt_ic_turbulent", "gmt_ct_step", "gmt_ct_cfl_async",
     "gmt_ct_divb_max", "gmt_ct_ic_orszag_tang", "gmt_ke_spectrum", "gmt_run", "gmt_ensemble_create", "gmt_ensemble_destroy",
     "gmt_ensemble_run", "gmt_density_pdf", "gmt_ke_band_loss", "gmt_adjoint_step", "gmt_adjoint_amp_grad",
     "gmt_adjoint_set_passes", "gmt_test_wait_limit", "march_nv", "march_nx", "march_nsp", "march_set_dtdx",
@@ -98,6 +98,8 @@ def lib():
             "gmt_forcing_set_modes": ([vp, C.POINTER(dbl), vp], C.c_int),
             "gmt_forcing_get_modes": ([vp, C.POINTER(dbl), vp], C.c_int),
             "gmt_forcing_counter": ([vp, C.POINTER(C.c_uint32)], C.c_int),
+            "gmt_forcing_get_state": ([vp, C.POINTER(dbl), C.POINTER(C.c_uint32), C.POINTER(dbl), vp], C.c_int),
+            "gmt_forcing_set_state": ([vp, C.POINTER(dbl), C.c_uint32, dbl, vp], C.c_int),
             "gmt_ic_orszag_tang": ([vp, vp, vp], C.c_int),
             "gmt_ic_uniform": ([vp, vp, dbl, dbl, dbl, dbl, dbl, vp], C.c_int),
             "gmt_ic_turbulent": ([vp, vp, dbl, dbl, dbl, dbl, dbl, dbl, dbl, C.c_uint32, vp], C.c_int),

@@ -75,6 +75,7 @@ struct gmt_ctx {
     double* modes = nullptr;  // [61][3][2]
     void* btab = nullptr;     // [nz][ny][24] reals
     void* trig[3] = {nullptr, nullptr, nullptr};
+    void* trig8 = nullptr;    // FP32: x table [nx][4][2] of 2 cos, -2 sin for the vectorised forcing kick
     void* ct_scratch = nullptr;
     void* fmass = nullptr;         // march with species: lower-face mass fluxes (3 planes)
     unsigned long long* divb = nullptr;
@@ -282,6 +283,7 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.iflo = p.iflo; A.use_llf = p.riemann == GMT_RIEMANN_LLF; A.do_turb = a->do_turb;
         A.btab = a->do_turb ? static_cast<const R*>(c->btab) : nullptr;
         A.trigx = static_cast<const R*>(c->trig[0]);
+        A.trig8 = static_cast<const R*>(c->trig8);
         A.cfl_out = nullptr;
         A.err = c->err;
         A.wait_cycles = c->wait_cycles;
@@ -314,6 +316,7 @@ int step_impl(gmt_ctx* c, const CPlanes<R>& u, const Planes<R>& o, const gmt_ste
         A.iflo = 0; A.use_llf = 0; A.do_turb = 0;
         A.btab = nullptr;
         A.trigx = static_cast<const R*>(c->trig[0]);
+        A.trig8 = static_cast<const R*>(c->trig8);
         A.cfl_out = nullptr;
         A.err = c->err;
         A.wait_cycles = c->wait_cycles;
@@ -511,6 +514,18 @@ int gmt_create(const gmt_params* p, gmt_ctx** out) {
         }
         if (e != cudaSuccess) { gmt_destroy(c); return cuda_fail(e, "trig upload"); }
     }
+    if (c->esize == 4) {
+        std::vector<double> t = trig_table(p->nx);
+        std::vector<float> t8((size_t)8 * p->nx);
+        for (int i = 0; i < p->nx; ++i)
+            for (int m = 0; m < 4; ++m) {
+                t8[(size_t)8 * i + 2 * m] = (float)(2.0 * t[(size_t)(2 * m) * p->nx + i]);
+                t8[(size_t)8 * i + 2 * m + 1] = (float)(-2.0 * t[(size_t)(2 * m + 1) * p->nx + i]);
+            }
+        cudaError_t e = cudaMalloc(&c->trig8, t8.size() * 4);
+        if (e == cudaSuccess) e = cudaMemcpy(c->trig8, t8.data(), t8.size() * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { gmt_destroy(c); return cuda_fail(e, "trig upload"); }
+    }
     int nd = p->turb_ndt > 0 ? p->turb_ndt : 100;
     double dtf = p->turb_T / nd;
     c->alpha = 1.0 - dtf / p->turb_T;
@@ -547,6 +562,7 @@ int gmt_destroy(gmt_ctx* c) {
     cudaFree(c->diag_out);
     cudaFree(c->modes);
     cudaFree(c->btab);
+    cudaFree(c->trig8);
     for (auto& t : c->trig) cudaFree(t);
     cudaFree(c->ct_scratch);
     cudaFree(c->fmass);
@@ -794,7 +810,7 @@ int gmt_adjoint_step(gmt_ctx* c, const void* u, const void* ubar_next, void* uba
         T.dt = A.dt; T.dtdx = A.dtdx; T.ch = A.ch; T.glm_fac = A.glm_fac; T.ramp = A.ramp;
         T.K = A.K;
         T.iflo = A.iflo; T.use_llf = A.use_llf; T.do_turb = A.do_turb;
-        T.btab = A.btab; T.trigx = A.trigx;
+        T.btab = A.btab; T.trigx = A.trigx; T.trig8 = static_cast<const R*>(c->trig8);
         T.cfl_out = nullptr;
         T.err = c->adj_err;
         T.wait_cycles = c->wait_cycles;
@@ -882,6 +898,25 @@ int gmt_forcing_get_modes(gmt_ctx* c, double* modes, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     GMT_CUDA(cudaMemcpyAsync(modes, c->modes, NMODES * 6 * sizeof(double), cudaMemcpyDeviceToHost, s));
     GMT_CUDA(cudaStreamSynchronize(s));
+    return GMT_OK;
+}
+
+int gmt_forcing_get_state(gmt_ctx* c, double* modes, uint32_t* counter, double* next_time, void* stream) {
+    if (!c || !modes || !counter || !next_time) return fail(GMT_ERR_ARG, "gmt_forcing_get_state: null argument");
+    int rc = gmt_forcing_get_modes(c, modes, stream);
+    if (rc) return rc;
+    *counter = c->counter;
+    *next_time = c->next_time;
+    return GMT_OK;
+}
+
+int gmt_forcing_set_state(gmt_ctx* c, const double* modes, uint32_t counter, double next_time, void* stream) {
+    if (!c || !modes) return fail(GMT_ERR_ARG, "gmt_forcing_set_state: null argument");
+    if (!std::isfinite(next_time)) return fail(GMT_ERR_ARG, "gmt_forcing_set_state: next_time must be finite");
+    int rc = gmt_forcing_set_modes(c, modes, stream);
+    if (rc) return rc;
+    c->counter = counter;
+    c->next_time = next_time;
     return GMT_OK;
 }
 
@@ -999,6 +1034,7 @@ cudaError_t run_enqueue(gmt_ctx* c, const void* src, void* dst, int flags, cudaS
     A.iflo = p.iflo; A.use_llf = p.riemann == GMT_RIEMANN_LLF; A.do_turb = (flags & GMT_RUN_FORCING) ? 1 : 0;
     A.btab = A.do_turb ? static_cast<const R*>(c->btab) : nullptr;
     A.trigx = static_cast<const R*>(c->trig[0]);
+    A.trig8 = static_cast<const R*>(c->trig8);
     A.cfl_out = c->cfl;
     A.err = c->err;
     A.wait_cycles = c->wait_cycles;
@@ -1141,6 +1177,7 @@ template <class R> int ens_bind(gmt_ensemble* E, void* const* u, void* const* w,
             a.do_turb = (flags & GMT_RUN_FORCING) ? 1 : 0;
             a.btab = a.do_turb ? static_cast<const R*>(E->btab[b]) : nullptr;
             a.trigx = static_cast<const R*>(E->trig[3 * b]);
+            a.trig8 = nullptr;
             a.cfl_out = E->cfl + 2 * b;
             a.err = E->err;
             a.wait_cycles = GMT_WAIT_CYCLES;

@@ -31,6 +31,7 @@ template <class R> struct UnsplitArgs {
     int iflo, use_llf, do_turb;
     const R* btab;         // forcing row table [nz][ny][4 kx][3 comp][2] (re, im) or null
     const R* trigx;        // [4 m][2 cos|sin][nx]
+    const R* trig8;        // FP32 or null: [nx][4 m][2 cos|sin] holding 2 cos and -2 sin (force_accel_f32)
     unsigned long long* cfl_out;  // [2] bits of non-negative doubles (max ctot, max signal) or null
     int* err;              // set to 1 when a bounded wait gives up (never expected)
     R dx;                  // cell size (dt/dx of device-supplied steps)
@@ -202,9 +203,9 @@ __device__ __forceinline__ void cfl_speeds(const Q9<R>& c, const Consts<R>& K, R
         const R c2 = K.gamma * q.v[4] * ir;
         const R b2 = (q.v[5] * q.v[5] + q.v[6] * q.v[6] + q.v[7] * q.v[7]) * ir;
         const R d2 = R(0.5) * (b2 + c2), t = c2 * ir;
-        sx = rabs(q.v[1]) + rsqrt_ieee(d2 + rsqrt_ieee(rmax(d2 * d2 - t * q.v[5] * q.v[5], R(0))));
-        sy = rabs(q.v[2]) + rsqrt_ieee(d2 + rsqrt_ieee(rmax(d2 * d2 - t * q.v[6] * q.v[6], R(0))));
-        sz = rabs(q.v[3]) + rsqrt_ieee(d2 + rsqrt_ieee(rmax(d2 * d2 - t * q.v[7] * q.v[7], R(0))));
+        sx = rabs(q.v[1]) + sqrt_r(d2 + sqrt_r(rmax(d2 * d2 - t * q.v[5] * q.v[5], R(0))));
+        sy = rabs(q.v[2]) + sqrt_r(d2 + sqrt_r(rmax(d2 * d2 - t * q.v[6] * q.v[6], R(0))));
+        sz = rabs(q.v[3]) + sqrt_r(d2 + sqrt_r(rmax(d2 * d2 - t * q.v[7] * q.v[7], R(0))));
     } else {
         sx = rabs(q.v[1]) + fast_speed(q, K.gamma, q.v[5]);
         sy = rabs(q.v[2]) + fast_speed(q, K.gamma, q.v[6]);
@@ -289,6 +290,29 @@ __device__ __forceinline__ void btab_row(const double* modes, const int* mode_k,
 #pragma unroll
         for (int c = 0; c < 3; ++c) { out[kx * 6 + 2 * c] = Br[c]; out[kx * 6 + 2 * c + 1] = Bi[c]; }
     }
+}
+
+// FP32 forcing acceleration with vectorised table loads: the row table's 24 values as six float4,
+// the x table (2 cos, -2 sin per m) as two float4, and 24 FMAs; the same sum as force_accel in
+// another order (FP32 round-off)
+__device__ __forceinline__ void force_accel_f32(const float* __restrict__ btab_row, const float* __restrict__ trig8,
+                                                int i, float ramp, float& ax, float& ay, float& az) {
+    const float4* t = reinterpret_cast<const float4*>(trig8 + 8 * i);
+    const float4 t0 = t[0], t1 = t[1];   // (2c0, -2s0, 2c1, -2s1), (2c2, -2s2, 2c3, -2s3)
+    const float4* b = reinterpret_cast<const float4*>(btab_row);
+    const float4 b0 = b[0], b1 = b[1], b2 = b[2], b3 = b[3], b4 = b[4], b5 = b[5];
+    // row layout [kx][component][re, im]
+    float S0 = fmaf(b0.x, t0.x, b0.y * t0.y), S1 = fmaf(b0.z, t0.x, b0.w * t0.y), S2 = fmaf(b1.x, t0.x, b1.y * t0.y);
+    S0 = fmaf(b1.z, t0.z, fmaf(b1.w, t0.w, S0));
+    S1 = fmaf(b2.x, t0.z, fmaf(b2.y, t0.w, S1));
+    S2 = fmaf(b2.z, t0.z, fmaf(b2.w, t0.w, S2));
+    S0 = fmaf(b3.x, t1.x, fmaf(b3.y, t1.y, S0));
+    S1 = fmaf(b3.z, t1.x, fmaf(b3.w, t1.y, S1));
+    S2 = fmaf(b4.x, t1.x, fmaf(b4.y, t1.y, S2));
+    S0 = fmaf(b4.z, t1.z, fmaf(b4.w, t1.w, S0));
+    S1 = fmaf(b5.x, t1.z, fmaf(b5.y, t1.w, S1));
+    S2 = fmaf(b5.z, t1.z, fmaf(b5.w, t1.w, S2));
+    ax = ramp * S0; ay = ramp * S1; az = ramp * S2;
 }
 
 // forcing acceleration at one cell from the per-row table (same order as the oracle)

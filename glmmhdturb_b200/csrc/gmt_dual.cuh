@@ -67,9 +67,9 @@ template <class R, int N> GMT_HD bool operator>=(const Dual<R, N>& a, const Dual
 template <class R, int N> GMT_HD Dual<R, N> rmax(const Dual<R, N>& a, const Dual<R, N>& b) { return a.v >= b.v ? a : b; }
 template <class R, int N> GMT_HD Dual<R, N> rmin(const Dual<R, N>& a, const Dual<R, N>& b) { return a.v <= b.v ? a : b; }
 template <class R, int N> GMT_HD Dual<R, N> rabs(const Dual<R, N>& a) { return a.v >= R(0) ? a : -a; }
-template <class R, int N> GMT_HD Dual<R, N> rsqrt_ieee(const Dual<R, N>& a) {
+template <class R, int N> GMT_HD Dual<R, N> sqrt_r(const Dual<R, N>& a) {
     Dual<R, N> r;
-    r.v = rsqrt_ieee(a.v);
+    r.v = sqrt_r(a.v);
     const R s = r.v > R(0) ? R(0.5) / r.v : R(0);
 #pragma unroll
     for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * s;

@@ -29,9 +29,9 @@ template <> GMT_HD double rmin(double a, double b) { return fmin(a, b); }
 template <class R> GMT_HD R rabs(R a);
 template <> GMT_HD float rabs(float a) { return fabsf(a); }
 template <> GMT_HD double rabs(double a) { return fabs(a); }
-template <class R> GMT_HD R rsqrt_ieee(R a);
-template <> GMT_HD float rsqrt_ieee(float a) { return sqrtf(a); }
-template <> GMT_HD double rsqrt_ieee(double a) { return sqrt(a); }
+template <class R> GMT_HD R sqrt_r(R a);
+template <> GMT_HD float sqrt_r(float a) { return sqrtf(a); }
+template <> GMT_HD double sqrt_r(double a) { return sqrt(a); }
 
 // Physical constants of one step, in working precision.
 template <class R> struct Consts {
@@ -72,7 +72,7 @@ template <class R> GMT_HD R fast_speed(const Q9<R>& q, R gamma, R bn) {
     R c2 = gamma * q.v[4] / rho;
     R b2 = (q.v[5] * q.v[5] + q.v[6] * q.v[6] + q.v[7] * q.v[7]) / rho;
     R d2 = R(0.5) * (b2 + c2);
-    return rsqrt_ieee(d2 + rsqrt_ieee(rmax(d2 * d2 - c2 * bn * bn / rho, R(0))));
+    return sqrt_r(d2 + sqrt_r(rmax(d2 * d2 - c2 * bn * bn / rho, R(0))));
 }
 
 // ideal-MHD x flux; F[Bx] and F[psi] are left 0 (glmmhd_turb.jl:98-115)
@@ -208,10 +208,11 @@ __device__ __forceinline__ void phys_flux_x2(const F2* q, F2 igm1, F2* f) {
 // F_D(m0 + a s) - F_D(m0 - a s), the two fluxes evaluated as one packed pair
 template <int D> __device__ __forceinline__ void flux_pair_diff(const Q9<float>& m0, const Q9<float>& s, F2 igm1,
                                                                float* d, float a = 1.0f) {
-    const F2 pm = {make_float2(a, -a)};
+    // the two states m0 + a s and m0 - a s, each formed by one scalar FMA straight into its half of
+    // the pair (the same single rounding as a packed FMA of splatted operands, without the copies)
     F2 q[9];
 #pragma unroll
-    for (int v = 0; v < 9; ++v) q[v] = fma2(splat2(s.v[v]), pm, splat2(m0.v[v]));
+    for (int v = 0; v < 9; ++v) q[v] = {make_float2(fmaf(a, s.v[v], m0.v[v]), fmaf(-a, s.v[v], m0.v[v]))};
     // rotate so that D is the x normal (rot_to): the velocity and field triples cycle
     constexpr int i1 = D == 0 ? 1 : (D == 1 ? 2 : 3), i2 = D == 0 ? 2 : (D == 1 ? 3 : 1), i3 = D == 0 ? 3 : (D == 1 ? 1 : 2);
     F2 r[9] = {q[0], q[i1], q[i2], q[i3], q[4], q[i1 + 4], q[i2 + 4], q[i3 + 4], q[8]};
@@ -323,8 +324,8 @@ GMT_HD Q9<R> llf_x(const Q9<R>& L, const Q9<R>& Rr, R gamma, R ch, R fbn, R fpsi
     R sL, sR;
     if (BOUND) {  // fast_speed_bound (glmmhd_turb.jl:307-310)
         R irL = R(1) / L.v[0], irR = R(1) / Rr.v[0];
-        sL = rabs(L.v[1]) + rsqrt_ieee((gamma * L.v[4] + L.v[5] * L.v[5] + L.v[6] * L.v[6] + L.v[7] * L.v[7]) * irL);
-        sR = rabs(Rr.v[1]) + rsqrt_ieee((gamma * Rr.v[4] + Rr.v[5] * Rr.v[5] + Rr.v[6] * Rr.v[6] + Rr.v[7] * Rr.v[7]) * irR);
+        sL = rabs(L.v[1]) + sqrt_r((gamma * L.v[4] + L.v[5] * L.v[5] + L.v[6] * L.v[6] + L.v[7] * L.v[7]) * irL);
+        sR = rabs(Rr.v[1]) + sqrt_r((gamma * Rr.v[4] + Rr.v[5] * Rr.v[5] + Rr.v[6] * Rr.v[6] + Rr.v[7] * Rr.v[7]) * irR);
     } else {
         sL = rabs(L.v[1]) + fast_speed(L, gamma, L.v[5]);
         sR = rabs(Rr.v[1]) + fast_speed(Rr, gamma, Rr.v[5]);
@@ -394,8 +395,6 @@ __device__ __forceinline__ Q9<float> hlld_x_f32(const Q9<float>& L, const Q9<flo
     const float d2L = 0.5f * fmaf(b2L, irL, c2L), d2R = 0.5f * fmaf(b2R, irR, c2R);
     const float cfL = sqrtf(d2L + sqrtf(fmaxf(fmaf(d2L, d2L, -c2L * bn2 * irL), 0.0f)));
     const float cfR = sqrtf(d2R + sqrtf(fmaxf(fmaf(d2R, d2R, -c2R * bn2 * irR), 0.0f)));
-    const float EL = fmaf(pL, igm1, fmaf(0.5f * dL, fmaf(uL, uL, fmaf(vL, vL, wL * wL)), 0.5f * b2L));
-    const float ER = fmaf(pR, igm1, fmaf(0.5f * dR, fmaf(uR, uR, fmaf(vR, vR, wR * wR)), 0.5f * b2R));
     const float cmax = fmaxf(cfL, cfR);
     const float SL = fminf(fminf(uL, uR) - cmax, 0.0f);
     const float SR = fmaxf(fmaxf(uL, uR) + cmax, 0.0f);
@@ -408,7 +407,8 @@ __device__ __forceinline__ Q9<float> hlld_x_f32(const Q9<float>& L, const Q9<flo
     const bool lside = SM >= 0.0f;
     const float sig = lside ? -1.0f : 1.0f;   // S*_s = SM + sig |bn| / sqrt(rho*_s)
     const float d = lside ? dL : dR, u = lside ? uL : uR, v = lside ? vL : vR, w = lside ? wL : wR;
-    const float by = lside ? byL : byR, bz = lside ? bzL : bzR, E = lside ? EL : ER, pt = lside ? ptL : ptR;
+    const float by = lside ? byL : byR, bz = lside ? bzL : bzR, pt = lside ? ptL : ptR;
+    const float E = fmaf(lside ? pL : pR, igm1, fmaf(0.5f * d, fmaf(u, u, fmaf(v, v, w * w)), 0.5f * (lside ? b2L : b2R)));
     const float S = lside ? SL : SR, a = lside ? aL : aR;
     const float isM = 1.0f / (S - SM);
     const float ds = fmaxf(a * isM, tiny);
@@ -497,7 +497,7 @@ template <class R> GMT_HD Q9<R> hlld_x(const Q9<R>& L, const Q9<R>& Rr, R gamma,
     R pts = ((SR - uR) * dR * ptL - (SL - uL) * dL * ptR + dL * dR * (SR - uR) * (SL - uL) * (uR - uL)) / den;
     R dLs = rmax(dL * (SL - uL) / (SL - SM), tiny);
     R dRs = rmax(dR * (SR - uR) / (SR - SM), tiny);
-    R sqdLs = rsqrt_ieee(dLs), sqdRs = rsqrt_ieee(dRs);
+    R sqdLs = sqrt_r(dLs), sqdRs = sqrt_r(dRs);
     R SLs = SM - rabs(bn) / sqdLs;
     R SRs = SM + rabs(bn) / sqdRs;
     Q9<R> f;

@@ -26,8 +26,8 @@ template <class R> GMT_HD void fast_speed_adj(const Q9<R>& q, R gamma, R bn, R c
     const R d2 = R(0.5) * (b2 + c2);
     const R disc = d2 * d2 - c2 * bn * bn / rho;
     const R dm = rmax(disc, R(0));
-    const R sd = rsqrt_ieee(dm);
-    const R cf = rsqrt_ieee(d2 + sd);
+    const R sd = sqrt_r(dm);
+    const R cf = sqrt_r(d2 + sd);
     const R t_b = cf > R(0) ? cb * (R(0.5) / cf) : R(0);
     R d2_b = t_b;
     const R dm_b = sd > R(0) ? t_b * (R(0.5) / sd) : R(0);
@@ -386,7 +386,7 @@ GMT_HD void hlld_x_adj(const Q9<R>& L, const Q9<R>& Rr, R gamma, R bn, const Q9<
     const R pts = (aR * sr.d * sl.pt - aL * sl.d * sr.pt + sl.d * sr.d * aR * aL * du) / den;
     const R qL = sl.d * aL / (sl.S - SM), qR = sr.d * aR / (sr.S - SM);
     const R dLs = rmax(qL, tiny), dRs = rmax(qR, tiny);
-    const R sqdLs = rsqrt_ieee(dLs), sqdRs = rsqrt_ieee(dRs);
+    const R sqdLs = sqrt_r(dLs), sqdRs = sqrt_r(dRs);
     const R abn = rabs(bn);
     const R SLs = SM - abn / sqdLs;
     const R SRs = SM + abn / sqdRs;

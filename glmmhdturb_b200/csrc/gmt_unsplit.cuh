@@ -27,6 +27,7 @@ namespace gmt {
 template <class R> struct Rec {
     Q9<R> m0, mh, s[3];
     bool up;
+    bool check;   // some lane of the warp may revert an interface state (warp-uniform)
 };
 
 // Shared-memory layout of the 9-variable arrays (the primitive ring, the interface states): an
@@ -89,6 +90,16 @@ __device__ __forceinline__ void recon_prims(const R* __restrict__ PR, int PN, in
     r.up = up;
     r.mh = cons2prim(hancock(r.m0, r.s[0], r.s[1], r.s[2], dtdx, K.gamma), K.gamma, K.smallr, K.pfl);
     if (r.mh.v[0] <= K.smallr || r.mh.v[4] <= K.pfl) r.mh = r.m0;
+    // PLM states are mh +- s_d, so some state of the cell has rho < smallr or p < pfl exactly when
+    // mh - max_d |s_d| does (mh - |s| is the smaller state, rounded alike); one warp vote then
+    // decides whether the per-state revert checks run at all.  PPM states are checked one by one.
+    bool bad = RECON == RECON_PPM;
+    if (RECON != RECON_PPM) {
+        const R dr = rmax(rmax(rabs(r.s[0].v[0]), rabs(r.s[1].v[0])), rabs(r.s[2].v[0]));
+        const R dp = rmax(rmax(rabs(r.s[0].v[4]), rabs(r.s[1].v[4])), rabs(r.s[2].v[4]));
+        bad = r.mh.v[0] - dr < K.smallr || r.mh.v[4] - dp < K.pfl;
+    }
+    r.check = __any_sync(__activemask(), bad);
 }
 
 // interface state of the reconstructed cell on the SIGN side of axis D
@@ -113,10 +124,12 @@ __device__ __forceinline__ Q9<R> face_state(const Rec<R>& r, const R* __restrict
     } else {
         f = padd(r.mh, r.s[D], SIGN > 0 ? R(1) : R(-1));
     }
-    // revert an unphysical state to the cell value; the revert is rare, so the 9 selects are
-    // skipped when no lane of the warp needs them
-    const bool bad = iflo && (f.v[0] < K.smallr || f.v[4] < K.pfl);
-    if (__any_sync(__activemask(), bad) && bad) f = r.m0;
+    // revert an unphysical state to the cell value; the revert is rare, so the checks are skipped
+    // when no lane of the warp can need them
+    if (iflo && r.check) {
+        const bool bad = f.v[0] < K.smallr || f.v[4] < K.pfl;
+        if (bad) f = r.m0;
+    }
     return f;
 }
 
@@ -455,7 +468,14 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
 #pragma unroll
                     for (int v = 0; v < 9; ++v) q.v[v] = A.u.p[v][g] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
                     R ax = R(0), ay = R(0), az = R(0);
-                    if (turb) force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
+                    if (turb) {
+                        if constexpr (std::is_same<R, float>::value) {
+                            if (A.trig8) force_accel_f32(A.btab + ((size_t)kf * ny + gy) * 24, A.trig8, gx, V.ramp, ax, ay, az);
+                            else force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
+                        } else {
+                            force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
+                        }
+                    }
                     if constexpr (S::kRecord) {
                         // the epilogue's adjoint at the pre-epilogue state q; R1bar and the identity
                         // part of ubar, and this cell's share of dL/d(amplitude)

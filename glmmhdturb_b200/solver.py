@@ -246,6 +246,24 @@ class Solver:
         check(lib().gmt_forcing_counter(self._ctx, C.byref(c)))
         return c.value
 
+    def forcing_state(self, stream=None) -> dict:
+        """The whole forcing state: modes, the Philox counter of the next OU update, next update time."""
+        m = np.zeros(_lib.NMODES * 6)
+        c = C.c_uint32()
+        nt = C.c_double()
+        check(lib().gmt_forcing_get_state(self._ctx, m.ctypes.data_as(C.POINTER(C.c_double)), C.byref(c),
+                                          C.byref(nt), _stream_handle(stream)))
+        return {"modes": m.reshape(_lib.NMODES, 3, 2), "counter": c.value, "next_time": nt.value}
+
+    def set_forcing_state(self, state: dict, stream=None):
+        """Restore a forcing_state() (from this or another context: the forcing is grid-independent)."""
+        m = np.ascontiguousarray(state["modes"], dtype=np.float64).reshape(-1)
+        if m.size != _lib.NMODES * 6:
+            raise ValueError("modes must have 61*3*2 entries")
+        check(lib().gmt_forcing_set_state(self._ctx, m.ctypes.data_as(C.POINTER(C.c_double)), int(state["counter"]),
+                                          float(state["next_time"]), _stream_handle(stream)))
+        self.next_time = float(state["next_time"])
+
     # ------------------------------------------------------------------ device-resident loop
     def run(self, u, w, nsteps, t0=0.0, t_end=1e300, *, ch_max_signal=True, forcing=False, graph=True, stream=None):
         """nsteps steps with dt, ch, glm_fac and the forcing cadence decided on the device (gmt_run);
@@ -256,6 +274,8 @@ class Solver:
         which = C.c_int32()
         check(lib().gmt_run(self._ctx, self._ptr(u), self._ptr(w), int(nsteps), float(t0), float(t_end), flags,
                             _stream_handle(stream), C.byref(t), C.byref(which)))
+        if forcing:
+            self.next_time = self.forcing_state(stream)["next_time"]
         return t.value, (w if which.value else u)
 
     # ------------------------------------------------------------------ initial conditions

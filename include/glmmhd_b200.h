@@ -219,6 +219,11 @@ int gmt_forcing_advance(gmt_ctx* ctx, void* stream);
 int gmt_forcing_set_modes(gmt_ctx* ctx, const double* modes, void* stream);
 int gmt_forcing_get_modes(gmt_ctx* ctx, double* modes, void* stream);
 int gmt_forcing_counter(gmt_ctx* ctx, uint32_t* counter);
+/* the whole forcing state: the modes, the Philox counter of the next OU update and the time of the
+ * next update (gmt_run's cadence), to checkpoint a run or carry it to another context or grid (the
+ * mode-sum forcing does not depend on the grid).  set_state also refreshes the mode table. */
+int gmt_forcing_get_state(gmt_ctx* ctx, double* modes, uint32_t* counter, double* next_time, void* stream);
+int gmt_forcing_set_state(gmt_ctx* ctx, const double* modes, uint32_t counter, double next_time, void* stream);
 
 /* --- initial conditions on the device ---------------------------------------------------- */
 int gmt_ic_orszag_tang(gmt_ctx* ctx, void* u, void* stream);            /* glmmhd_turb.jl:2021 */

@@ -75,3 +75,47 @@ def test_ct_fullsize_divergence_roundoff():
     print(f"CT 512^3 FP32 max |div B|: initial {d0:.3e}, after two steps {d1:.3e}")
     assert torch.isfinite(q).all()
     assert d0 < 1e-3 and d1 < 1e-3, (d0, d1)
+
+
+def test_configs4_1024cube_forward_20_steps():
+    """The large-scale forward configuration: 1024^3 FP32, PLM-MC + HLLD + GLM with forcing, from the
+    uniform state (rho 1, p 0.6, B0 = (0.775, 0, 0)) with the forcing amplitude 4x the Mach-1
+    calibration (stationary rms Mach ~2: v^2 grows with the amplitude), seed 2; 20 steps, two
+    registers of 38.7 GB.  Checks a finite state, mass conservation by the flux form, and the
+    throughput (CUDA events over the 20 steps, printed; at least 9 Gzone/s)."""
+    import json
+    from glmmhdturb_b200 import Solver
+    from tests.golden import make_golden as G
+    torch.cuda.empty_cache()
+    n = 1024
+    amp = 4.0 * G.calibrated_amp()
+    s = Solver(n, dtype="f32", gamma=5 / 3, courant=0.3, turb_amp=amp, turb_T=0.5, turb_ndt=100, turb_seed=2,
+               tile=(32, 16, 0))
+    u, w = s.alloc(), s.alloc()
+    s.ic_uniform(u, 1.0, 0.6, (0.775, 0.0, 0.0))
+    mass0 = s.diagnostics(u)["mass"]
+    s.forcing_reset()
+    s.forcing_advance()
+    t = 0.0
+    cm, sm = s.cfl(u)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(20):
+        while t >= s.next_time:
+            s.forcing_advance()
+        dt = min(0.3 * s.dx / cm, s.next_time - t)
+        s.step(u, w, dt, t=t, ch=sm, glm_fac=math.exp(-(sm / 0.18) * dt), do_turb=True, want_cfl=True)
+        cm, sm = s.cfl_result()
+        u, w = w, u
+        t += dt
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 20
+    d = s.diagnostics(u)
+    rate = n ** 3 / (ms * 1e-3)
+    print(json.dumps({"configs4_forward_1024": {"ms_per_step": ms, "gzone_per_s": rate / 1e9, "t": t,
+                                                "vrms": d["vrms"], "mass_rel_change": d["mass"] / mass0 - 1}}))
+    assert d["finite"] and abs(d["mass"] / mass0 - 1.0) <= 1e-5
+    assert rate >= 9e9, ms
+    del u, w, s
+    torch.cuda.empty_cache()

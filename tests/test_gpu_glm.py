@@ -119,7 +119,9 @@ def test_nonfinite_state_reports_error(golden):
 # HLLD, ch = global max fast signal speed, c_p^2/c_h = 0.18, OU modes 1<=|k|<=3, tau=0.5, seed 0,
 # CFL 0.3, 100 steps; all 9 fields against the oracle.
 # ---------------------------------------------------------------------------------------------
-CFG0_AMP = 2.0   # forcing amplitude (stationary rms acceleration), frozen for configs[0]
+# forcing amplitude (stationary rms acceleration) calibrated so that the rms Mach number reaches 1 at
+# t = 2 tau (tests/golden/calibrate_amp.py, bisection with the FP64 oracle at 64^3)
+CFG0_AMP = G.calibrated_amp()
 
 
 @pytest.fixture(scope="module")
@@ -184,9 +186,10 @@ def test_config0_fp32_100_steps_error(config0_oracle):
     print("configs[0] FP32 per-field max rel err after 100 steps:", ["%.2e" % e for e in errs])
     print("configs[0] FP32 per-field relL2 after 100 steps:", ["%.2e" % e for e in rel2])
     # rho, momentum, E, B: FP32 round-off of O(0.01) perturbations on an O(1) background; psi is a
-    # small cleaning field sourced by round-off-level div B, so its field-scale error is larger
-    assert max(errs[:8]) <= 1e-4 and max(rel2[:8]) <= 1e-4, (errs, rel2)
-    assert errs[8] <= 5e-2, (errs, rel2)
+    # small cleaning field sourced by round-off-level div B, so its field-scale error is larger.
+    # Measured (calibrated amplitude): field-scale max 1.44e-5 (By), relL2 8.6e-6; psi 3.4e-3 / 4.8e-3
+    assert max(errs[:8]) <= 3e-5 and max(rel2[:8]) <= 1.5e-5, (errs, rel2)
+    assert errs[8] <= 1e-2 and rel2[8] <= 1e-2, (errs, rel2)
 
 
 def test_orszag_tang_gpu_fp32_pin():

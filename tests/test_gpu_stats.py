@@ -80,3 +80,43 @@ def test_density_pdf_matches_numpy(oracle, dtype):
     assert abs(st["sigma_s"] - sv.std()) <= 1e-10 * sv.std()
     again, st2 = s.density_pdf(ud, nbins=40, smin=-2.0, smax=2.0)
     assert np.array_equal(again, pdf) and st2 == st    # deterministic
+
+
+def test_checkpoint_restart_continues_the_run_bit_for_bit(tmp_path):
+    """A forced device-loop run split by a checkpoint (state and the whole forcing state: modes, OU
+    counter, next update time) into a fresh context equals the unsplit run bit for bit."""
+    from glmmhdturb_b200 import Solver, checkpoint
+    kw = dict(dtype="f32", gamma=5 / 3, courant=0.3, turb_amp=3.0, turb_T=0.5, turb_ndt=100, turb_seed=5)
+    a = Solver(32, **kw)
+    u, w = a.alloc(), a.alloc()
+    a.ic_turbulent(u, mach=1.0, seed=2)
+    u0 = u.clone()
+    a.forcing_reset()
+    t, res = a.run(u, w, 40, forcing=True, graph=False)
+    want = res.clone()
+    b = Solver(32, **kw)
+    u.copy_(u0)
+    b.forcing_reset()
+    t1, res = b.run(u, w, 20, forcing=True, graph=False)
+    path = str(tmp_path / "half.gmt")
+    checkpoint.save(path, res, t=t1, step=20, solver=b)
+    v, h = checkpoint.load(path)
+    c = Solver(32, **kw)
+    checkpoint.restore_forcing(c, h)
+    assert c.forcing_state()["counter"] == b.forcing_state()["counter"] > 0
+    w2 = torch.empty_like(v)
+    t2, res2 = c.run(v, w2, 20, t0=h["t"], forcing=True, graph=False)
+    assert t2 == t and torch.equal(res2, want)
+
+
+def test_spinup_levels_reaches_the_target_on_every_grid():
+    from glmmhdturb_b200 import checkpoint
+    u, t, info, s = checkpoint.spinup_levels(64, n0=16, seed=1, amp=3.7737, mach_target=0.6, mach_coarse=0.9,
+                                             dt_level=0.02, t_max=3.0, chunk=20)
+    assert [m for m, *_ in info] == [16, 32, 64]
+    assert all(b[1] > a[1] for a, b in zip(info, info[1:]))          # time advances through the ladder
+    assert info[0][3] >= 0.54 and info[-1][3] >= 0.6 and t < 3.0
+    d = s.diagnostics(u)
+    assert d["finite"] and abs(d["vrms"] / np.sqrt(5 / 3 * 0.6) - info[-1][3]) < 1e-12
+    assert s.forcing_state()["counter"] > 0
+    assert u.shape == (9, 64, 64, 64)
