@@ -2,10 +2,11 @@
 // per-cell passes (CTMHD.step!, ct_mhd.jl:174; the fused march of spike_ctm.cu:250-298).
 //
 // Pass A (ct_tile_kernel): a block owns an OX x OY column tile over LZ planes, exactly like the
-// GLM step.  Shared memory holds
-//   PR[3][9][(OX+4)(OY+4)]  cell primitives with the face-averaged field (ring of 3 planes),
+// GLM step.  Shared memory holds (9-variable arrays in the Lay layout of the GLM tile march: FP32
+// cells as two 16-byte vectors and a scalar)
+//   PR[3][(OX+4)(OY+4)]     cell primitives with the face-averaged field (ring of 3 planes),
 //   FB[3][3][(OX+4)(OY+4)]  the lower-face fields bxf, byf, bzf of the same cells,
-//   ST[4][9][(OX+2)(OY+2)]  in-plane interface states, overwritten by the face fluxes,
+//   ST[4][(OX+2)(OY+2)]     in-plane interface states, overwritten by the face fluxes,
 //   SG[9][(OY+5)][OX+8]     staging of plane k+2: 5 conserved, bxf, byf, bzf(k+2), bzf(k+3)
 // (one more row and column than the ring, for the face averages of the outermost cells, at column
 // offset 2; tiles clear of the box edges fill it by two TMA copies, the others by cp.async).  Per
@@ -48,7 +49,7 @@ enum CTScratch {
 // byte offset of the reduction / mbarrier words: after the real arrays, rounded up to 16 bytes
 // staging plane: 128-byte aligned (a TMA destination), after the rings and the states
 template <class R> __host__ __device__ inline size_t ct_tile_sg_offset(int ox, int oy) {
-    size_t PN = (size_t)(ox + 4) * (oy + 4), RN = (size_t)(ox + 2) * (oy + 2);
+    size_t PN = (size_t)lay_n<R>((ox + 4) * (oy + 4)), RN = (size_t)lay_n<R>((ox + 2) * (oy + 2));
     return ((27 * PN + 9 * PN + 36 * RN) * sizeof(R) + 127) / 128 * 128;
 }
 template <class R> __host__ __device__ inline size_t ct_tile_words_offset(int ox, int oy) {
@@ -82,8 +83,9 @@ __device__ __forceinline__ void ct_stage_plane(R* __restrict__ SG, const CPlanes
 // staged plane -> primitives with the face-averaged field (ct_mhd.jl:85-97) and the lower faces
 template <class R>
 __device__ __forceinline__ void ct_unstage_plane(R* __restrict__ PRs, R* __restrict__ FBs, const R* __restrict__ SG,
-                                                 int PN, int PW, int SN5, int SW, const Consts<R>& K, int tid, int nt) {
-    for (int c = tid; c < PN; c += nt) {
+                                                 int PN, int PNc, int PW, int SN5, int SW, const Consts<R>& K, int tid,
+                                                 int nt) {
+    for (int c = tid; c < PNc; c += nt) {
         const int lx = c % PW, ly = c / PW;
         const int c5 = ly * SW + lx + 2;
         Q9<R> cu;
@@ -95,8 +97,7 @@ __device__ __forceinline__ void ct_unstage_plane(R* __restrict__ PRs, R* __restr
         cu.v[7] = R(0.5) * (bzl + SG[8 * SN5 + c5]);
         cu.v[8] = R(0);
         const Q9<R> q = cons2prim(cu, K.gamma, K.smallr, K.smallp);
-#pragma unroll
-        for (int v = 0; v < 9; ++v) PRs[v * PN + c] = q.v[v];
+        Lay<R>::put(PRs, PN, c, q);
         FBs[0 * PN + c] = bxl;
         FBs[1 * PN + c] = byl;
         FBs[2 * PN + c] = bzl;
@@ -114,8 +115,8 @@ __device__ __forceinline__ void ct_neighbours(const R* PR, int PN, int PW, int c
     const R* PL = PR + (size_t)(D == 2 ? sm : s0) * 9 * PN;
     const R* PP = PR + (size_t)(D == 2 ? sp : s0) * 9 * PN;
     const int cl = D == 0 ? c - 1 : (D == 1 ? c - PW : c), cr = D == 0 ? c + 1 : (D == 1 ? c + PW : c);
-#pragma unroll
-    for (int v = 0; v < 9; ++v) { L.v[v] = PL[v * PN + cl]; Rr.v[v] = PP[v * PN + cr]; }
+    L = Lay<R>::get(PL, PN, cl);
+    Rr = Lay<R>::get(PP, PN, cr);
 }
 
 template <int D, class R>
@@ -166,10 +167,11 @@ __device__ __forceinline__ Q9<R> ct_flux(const Q9<R>& L, const Q9<R>& Rr, const 
 template <class R, int RECON, int RIEM, int TOX, int TOY>
 __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int bz, unsigned char* smem_raw) {
     const int OX = TOX > 0 ? TOX : A.ox, OY = TOY > 0 ? TOY : A.oy;
-    const int PW = OX + 4, PN = (OX + 4) * (OY + 4);
+    const int PW = OX + 4, PN = lay_n<R>((OX + 4) * (OY + 4));   // padded array lengths (Lay layout)
+    const int PNc = (OX + 4) * (OY + 4);                           // ring cells per plane
     const int PW5 = OX + 5, PN5 = (OX + 5) * (OY + 5);
     const int SW = OX + 8, SN5 = (OX + 8) * (OY + 5);
-    const int RW = OX + 2, RN = (OX + 2) * (OY + 2);
+    const int RW = OX + 2, RN = lay_n<R>((OX + 2) * (OY + 2));
     R* PR = reinterpret_cast<R*>(smem_raw);
     R* FB = PR + 27 * PN;
     R* ST = FB + 9 * PN;
@@ -207,8 +209,8 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
         ct_stage_plane(SG, A.q, PN5, PW5, SW, SN5, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
         cp_async_wait_all();
         __syncthreads();
-        ct_unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, FB + mod3(z0 - 2 + j) * 3 * PN, SG, PN, PW, SN5, SW, K, tid,
-                         NT);
+        ct_unstage_plane(PR + mod3(z0 - 2 + j) * 9 * PN, FB + mod3(z0 - 2 + j) * 3 * PN, SG, PN, PNc, PW, SN5, SW, K,
+                         tid, NT);
         if (j == 2 && tid == 0) {
             mbar_init(mbar, tma ? 1u : (unsigned)NT);
             if (tma) fence_mbar_init();
@@ -249,27 +251,23 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
         {
             Q9<R> XY, Fxl, Fyl;
             if (kr - 1 >= z0) {
-                Fxl = st_get(ST + 1 * 9 * RN, RN, rown);
-                Fyl = st_get(ST + 3 * 9 * RN, RN, rown);
+                Fxl = Lay<R>::get(ST + 1 * 9 * RN, RN, rown);
+                Fyl = Lay<R>::get(ST + 3 * 9 * RN, RN, rown);
 #pragma unroll
                 for (int v = 0; v < 9; ++v) XY.v[v] = (Fxl.v[v] - Fxh.v[v]) + (Fyl.v[v] - Fyh.v[v]);
             }
             CTCell<R> r;
-            {
-                const R* P0 = PR + (size_t)s0 * 9 * PN;
-#pragma unroll
-                for (int v = 0; v < 9; ++v) r.m0.v[v] = P0[v * PN + cown];
-            }
+            r.m0 = Lay<R>::get(PR + (size_t)s0 * 9 * PN, PN, cown);
             if (!first && !last) {
                 ct_prep<0>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx, A.halfslope);
-                st_put(ST + 0 * 9 * RN, RN, rown,
+                Lay<R>::put(ST + 0 * 9 * RN, RN, rown,
                        ct_state<0, +1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[0 * PN + cown + 1]));
-                st_put(ST + 1 * 9 * RN, RN, rown,
+                Lay<R>::put(ST + 1 * 9 * RN, RN, rown,
                        ct_state<0, -1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[0 * PN + cown]));
                 ct_prep<1>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx, A.halfslope);
-                st_put(ST + 2 * 9 * RN, RN, rown,
+                Lay<R>::put(ST + 2 * 9 * RN, RN, rown,
                        ct_state<1, +1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[1 * PN + cown + PW]));
-                st_put(ST + 3 * 9 * RN, RN, rown,
+                Lay<R>::put(ST + 3 * 9 * RN, RN, rown,
                        ct_state<1, -1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[1 * PN + cown]));
             }
             ct_prep<2>(r, PR, PN, PW, cown, s0, sm, sp, K, dtdx, A.halfslope);
@@ -286,8 +284,9 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
 #pragma unroll
                     for (int v = 0; v < 5; ++v) q.v[v] = A.q.p[v][g] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
                     // the epilogue sees the old cell-centred field
-                    const R vx = Pm[1 * PN + cown], vy = Pm[2 * PN + cown], vz = Pm[3 * PN + cown];
-                    const R bxc = Pm[5 * PN + cown], byc = Pm[6 * PN + cown], bzc = Pm[7 * PN + cown];
+                    const Q9<R> pm = Lay<R>::get(Pm, PN, cown);
+                    const R vx = pm.v[1], vy = pm.v[2], vz = pm.v[3];
+                    const R bxc = pm.v[5], byc = pm.v[6], bzc = pm.v[7];
                     q.v[5] = bxc; q.v[6] = byc; q.v[7] = bzc; q.v[8] = R(0);
                     R ax = R(0), ay = R(0), az = R(0);
                     if (turb) force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, A.ramp, ax, ay, az);
@@ -321,11 +320,7 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
                 else if (h < 2 * OY + OX) { int f = h - 2 * OY; rc = (f + 1); cc = (f + 2) + PW * 1; which = 2; }
                 else { int f = h - 2 * OY - OX; rc = (f + 1) + RW * (OY + 1); cc = (f + 2) + PW * (OY + 2); which = 3; }
                 CTCell<R> r;
-                {
-                    const R* P0 = PR + (size_t)s0 * 9 * PN;
-#pragma unroll
-                    for (int v = 0; v < 9; ++v) r.m0.v[v] = P0[v * PN + cc];
-                }
+                r.m0 = Lay<R>::get(PR + (size_t)s0 * 9 * PN, PN, cc);
                 Q9<R> f;
                 if (which < 2) {
                     ct_prep<0>(r, PR, PN, PW, cc, s0, sm, sp, K, dtdx, A.halfslope);
@@ -336,31 +331,31 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
                     if (which == 2) f = ct_state<1, +1, RECON>(r, PR, PN, PW, cc, s0, sm, sp, K, FB0[1 * PN + cc + PW]);
                     else f = ct_state<1, -1, RECON>(r, PR, PN, PW, cc, s0, sm, sp, K, FB0[1 * PN + cc]);
                 }
-                st_put(ST + which * 9 * RN, RN, rc, f);
+                Lay<R>::put(ST + which * 9 * RN, RN, rc, f);
             }
         }
         __syncthreads();
         if (!first && !last) {
-            Fxh = ct_flux<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, rown), st_get(ST + 1 * 9 * RN, RN, ixh), K);
-            st_put(ST + 1 * 9 * RN, RN, ixh, Fxh);
-            Fyh = ct_flux<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, rown), st_get(ST + 3 * 9 * RN, RN, iyh), K);
-            st_put(ST + 3 * 9 * RN, RN, iyh, Fyh);
+            Fxh = ct_flux<0, RIEM>(Lay<R>::get(ST + 0 * 9 * RN, RN, rown), Lay<R>::get(ST + 1 * 9 * RN, RN, ixh), K);
+            Lay<R>::put(ST + 1 * 9 * RN, RN, ixh, Fxh);
+            Fyh = ct_flux<1, RIEM>(Lay<R>::get(ST + 2 * 9 * RN, RN, rown), Lay<R>::get(ST + 3 * 9 * RN, RN, iyh), K);
+            Lay<R>::put(ST + 3 * 9 * RN, RN, iyh, Fyh);
             for (int h = NT - 1 - tid; h < OX + OY; h += NT) {
                 if (h < OY) {
                     const int il = 0 + RW * (h + 1), ir = 1 + RW * (h + 1);
-                    st_put(ST + 1 * 9 * RN, RN, ir, ct_flux<0, RIEM>(st_get(ST + 0 * 9 * RN, RN, il), st_get(ST + 1 * 9 * RN, RN, ir), K));
+                    Lay<R>::put(ST + 1 * 9 * RN, RN, ir, ct_flux<0, RIEM>(Lay<R>::get(ST + 0 * 9 * RN, RN, il), Lay<R>::get(ST + 1 * 9 * RN, RN, ir), K));
                 } else {
                     const int c = h - OY;
                     const int il = (c + 1), ir = (c + 1) + RW;
-                    st_put(ST + 3 * 9 * RN, RN, ir, ct_flux<1, RIEM>(st_get(ST + 2 * 9 * RN, RN, il), st_get(ST + 3 * 9 * RN, RN, ir), K));
+                    Lay<R>::put(ST + 3 * 9 * RN, RN, ir, ct_flux<1, RIEM>(Lay<R>::get(ST + 2 * 9 * RN, RN, il), Lay<R>::get(ST + 3 * 9 * RN, RN, ir), K));
                 }
             }
         }
         if (load) {
             mbar_wait(mbar, phase, A.err, A.wait_cycles);
             phase ^= 1u;
-            ct_unstage_plane(PR + mod3(kr + 2) * 9 * PN, FB + mod3(kr + 2) * 3 * PN, SG, PN, PW, SN5, SW, K,
-                             tid < nunst ? tid : PN, nunst);
+            ct_unstage_plane(PR + mod3(kr + 2) * 9 * PN, FB + mod3(kr + 2) * 3 * PN, SG, PN, PNc, PW, SN5, SW, K,
+                             tid < nunst ? tid : PNc, nunst);
         }
         __syncthreads();
     }
