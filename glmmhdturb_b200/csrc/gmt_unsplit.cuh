@@ -8,7 +8,9 @@
 //   ST[4][(OX+2)(OY+2)]     in-plane interface states +x,-x,+y,-y of the reconstruction region,
 //                           overwritten in place by the face fluxes,
 //   SG[9][(OY+4)][OX+8]     conserved staging plane k+2 (the ring region at column offset 2),
-//                           filled while plane k computes.
+//                           filled while plane k computes,
+//   TS[OX][8], BS[OY][24]   FP32: the forcing kick's x table of the tile's columns and row table
+//                           of its rows for the plane written next.
 // Each owned thread keeps its column's z-face work in registers (the +z state of plane k-1 and
 // F_z at its lower face) plus its own x/y face fluxes, so every face is solved once, every cell is
 // read from HBM once and written once, and a plane costs two block barriers.  The next conserved
@@ -183,7 +185,8 @@ __device__ __forceinline__ void unstage_plane(R* __restrict__ PRs, const R* __re
 }
 
 // shared-memory layout of the tile march: PR ring, ST states, then (128-byte aligned, as a TMA
-// destination) the staging plane SG, then (16-byte aligned) the reduction and mbarrier words
+// destination) the staging plane SG, then (16-byte aligned) the reduction and mbarrier words and,
+// in FP32, the tile's forcing tables (8 floats per column, 24 per row)
 template <class R> __host__ __device__ inline size_t unsplit_sg_offset(int ox, int oy) {
     size_t PN = (size_t)lay_n<R>((ox + 4) * (oy + 4)), RN = (size_t)lay_n<R>((ox + 2) * (oy + 2));
     return ((27 * PN + 36 * RN) * sizeof(R) + 127) / 128 * 128;
@@ -193,7 +196,7 @@ template <class R> __host__ __device__ inline size_t unsplit_red_offset(int ox, 
     return (unsplit_sg_offset<R>(ox, oy) + 9 * SN * sizeof(R) + 15) / 16 * 16;
 }
 template <class R> __host__ __device__ inline size_t unsplit_smem_bytes(int ox, int oy) {
-    return unsplit_red_offset<R>(ox, oy) + 40 * sizeof(double);
+    return unsplit_red_offset<R>(ox, oy) + 40 * sizeof(double) + (sizeof(R) == 4 ? 32 * (size_t)ox + 96 * (size_t)oy : 0);
 }
 
 // adjoint record mode: interface state k (+x, -x, +y, -y, +z, -z) of cell g
@@ -319,6 +322,10 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     R* ST = PR + 27 * PN;
     R* SG = reinterpret_cast<R*>(smem_raw + unsplit_sg_offset<R>(OX, OY));
     double* red = reinterpret_cast<double*>(smem_raw + unsplit_red_offset<R>(OX, OY));
+    // FP32 forcing tables of the tile: the x table of its columns (staged once) and the row table
+    // of its rows for the plane written next (staged in the phase before that write-out)
+    float* TS = reinterpret_cast<float*>(smem_raw + unsplit_red_offset<R>(OX, OY) + 40 * sizeof(double));
+    float* BS = TS + 8 * OX;
 
     const int tid = threadIdx.x, NT = OX * OY;
     const int tx = tid % OX, ty = tid / OX;
@@ -348,6 +355,10 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     }
     const unsigned tma_bytes = (unsigned)(9 * SN * sizeof(R));
 
+    if constexpr (std::is_same<R, float>::value && !OVERHANG) {
+        if (A.trig8 && tid < 2 * OX)
+            reinterpret_cast<float4*>(TS)[tid] = reinterpret_cast<const float4*>(A.trig8 + 8 * (size_t)x0)[tid];
+    }
     // prologue: primitives of planes z0-2, z0-1, z0
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
     for (int j = 0; j < 3; ++j) {
@@ -458,19 +469,30 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
             Q9<R> Pz = S::template state<2, +1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
             if (!first && !last) record(4, Pz);
             if (!first) {
+                // the old state of the cell written out below, loaded before the z-face solve so that
+                // the solve hides its latency
+                const bool wr = kr - 1 >= z0;
+                const int kf = kr - 1;
+                const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * (wr ? kf : 0));
+                Q9<R> u0;
+#pragma unroll
+                for (int v = 0; v < 9; ++v) u0.v[v] = wr ? __ldg(A.u.p[v] + g) : R(0);
                 Q9<R> Mz = S::template state<2, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
                 if (!last) record(5, Mz);
                 Q9<R> Fzhi = S::template flux<2>(pPz, Mz, K, ch, A.use_llf != 0);
-                if (kr - 1 >= z0) {
-                    const int kf = kr - 1;
-                    const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * kf);
+                if (wr) {
                     Q9<R> q;
 #pragma unroll
-                    for (int v = 0; v < 9; ++v) q.v[v] = A.u.p[v][g] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
+                    for (int v = 0; v < 9; ++v) q.v[v] = u0.v[v] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
                     R ax = R(0), ay = R(0), az = R(0);
                     if (turb) {
                         if constexpr (std::is_same<R, float>::value) {
-                            if (A.trig8) force_accel_f32(A.btab + ((size_t)kf * ny + gy) * 24, A.trig8, gx, V.ramp, ax, ay, az);
+                            if (A.trig8) {
+                                if constexpr (OVERHANG)
+                                    force_accel_f32(A.btab + ((size_t)kf * ny + gy) * 24, A.trig8, gx, V.ramp, ax, ay, az);
+                                else
+                                    force_accel_f32(BS + 24 * ty, TS, tx, V.ramp, ax, ay, az);
+                            }
                             else force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
                         } else {
                             force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
@@ -560,6 +582,12 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
                     Lay<R>::put(ST + 3 * 9 * RN, RN, ir, F);
                 }
             }
+        }
+        // the forcing row table of the tile's rows for plane kr, written out in the next phase R
+        if constexpr (std::is_same<R, float>::value && !OVERHANG) {
+            if (turb && A.trig8 && kr >= z0 && kr < z1 && tid < 6 * OY)
+                reinterpret_cast<float4*>(BS)[tid] =
+                    reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + y0) * 24)[tid];
         }
         if (load) {
             mbar_wait(mbar, phase, A.err, A.wait_cycles);
