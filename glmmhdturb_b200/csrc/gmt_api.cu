@@ -391,6 +391,7 @@ int ct_step_impl(gmt_ctx* c, const CPlanes8<R>& q, const Planes8<R>& o, const gm
     A.do_turb = a->do_turb;
     A.btab = a->do_turb ? static_cast<const R*>(c->btab) : nullptr;
     A.trigx = static_cast<const R*>(c->trig[0]);
+    A.trig8 = static_cast<const R*>(c->trig8);
     A.scratch = static_cast<R*>(c->ct_scratch);
     A.err = c->err;
     A.wait_cycles = c->wait_cycles;

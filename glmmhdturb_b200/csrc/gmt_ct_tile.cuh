@@ -8,8 +8,11 @@
 //   FB[3][3][(OX+4)(OY+4)]  the lower-face fields bxf, byf, bzf of the same cells,
 //   ST[4][(OX+2)(OY+2)]     in-plane interface states, overwritten by the face fluxes,
 //   SG[9][(OY+5)][OX+8]     staging of plane k+2: 5 conserved, bxf, byf, bzf(k+2), bzf(k+3)
-// (one more row and column than the ring, for the face averages of the outermost cells, at column
-// offset 2; tiles clear of the box edges fill it by two TMA copies, the others by cp.async).  Per
+//   TS[OX][8], BS[OY][24]   FP32: the forcing kick's x table of the tile's columns and row table
+//                           of its rows for the plane written next
+// (SG has one more row and column than the ring, for the face averages of the outermost cells, at
+// column offset 2; tiles clear of the box edges fill it by two TMA copies, the others by
+// cp.async).  The write-out's old cell state is loaded before the z-face solve.  Per
 // direction each cell gets a full (or ct_mhd.jl's half) MonCen slope, the transverse-free 1-D
 // Hancock predictor and its two face states, whose normal component is the face field; every
 // face is solved once (HLL or HLLD, no GLM).  The write-out does the hydro update with the
@@ -57,7 +60,7 @@ template <class R> __host__ __device__ inline size_t ct_tile_words_offset(int ox
     return (ct_tile_sg_offset<R>(ox, oy) + 9 * SN5 * sizeof(R) + 15) / 16 * 16;
 }
 template <class R> __host__ __device__ inline size_t ct_tile_smem_bytes(int ox, int oy) {
-    return ct_tile_words_offset<R>(ox, oy) + 40 * sizeof(double);
+    return ct_tile_words_offset<R>(ox, oy) + 40 * sizeof(double) + (sizeof(R) == 4 ? 32 * (size_t)ox + 96 * (size_t)oy : 0);
 }
 
 // stage plane kp: the conserved cell variables, the three face fields at kp and bzf at kp+1, on
@@ -177,6 +180,10 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
     R* ST = FB + 9 * PN;
     R* SG = reinterpret_cast<R*>(smem_raw + ct_tile_sg_offset<R>(OX, OY));
     double* red = reinterpret_cast<double*>(smem_raw + ct_tile_words_offset<R>(OX, OY));
+    // FP32 forcing tables of the tile: the x table of its columns (staged once) and the row table
+    // of its rows for the plane written next (staged in the phase before that write-out)
+    float* TS = reinterpret_cast<float*>(smem_raw + ct_tile_words_offset<R>(OX, OY) + 40 * sizeof(double));
+    float* BS = TS + 8 * OX;
 
     const int tid = threadIdx.x, NT = OX * OY;
     const int tx = tid % OX, ty = tid / OX;
@@ -204,6 +211,11 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
     }
     const unsigned tma_bytes = (unsigned)(9 * SN5 * sizeof(R));
 
+    if constexpr (std::is_same<R, float>::value) {
+        if (A.trig8)
+            for (int i = tid; i < 2 * OX; i += NT)
+                reinterpret_cast<float4*>(TS)[i] = reinterpret_cast<const float4*>(A.trig8 + 8 * (size_t)x0)[i];
+    }
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
     for (int j = 0; j < 3; ++j) {
         ct_stage_plane(SG, A.q, PN5, PW5, SW, SN5, x0, y0, z0 - 2 + j, nx, ny, nz, tid, NT);
@@ -274,22 +286,35 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
             const R* FBp = FB + (size_t)sp * 3 * PN;
             Q9<R> Pz = ct_state<2, +1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FBp[2 * PN + cown]);
             if (!first) {
+                // the old cell state written out below, loaded before the z-face solve so that the
+                // solve hides its latency
+                const bool wr = kr - 1 >= z0;
+                const int kf = kr - 1;
+                const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * (wr ? kf : 0));
+                R u0[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) u0[v] = wr ? __ldg(A.q.p[v] + g) : R(0);
                 Q9<R> Mz = ct_state<2, -1, RECON>(r, PR, PN, PW, cown, s0, sm, sp, K, FB0[2 * PN + cown]);
                 Q9<R> Fzhi = ct_flux<2, RIEM>(pPz, Mz, K);
-                if (kr - 1 >= z0) {
-                    const int kf = kr - 1;
-                    const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * kf);
+                if (wr) {
                     const R* Pm = PR + (size_t)sm * 9 * PN;
                     Q9<R> q;
 #pragma unroll
-                    for (int v = 0; v < 5; ++v) q.v[v] = A.q.p[v][g] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
+                    for (int v = 0; v < 5; ++v) q.v[v] = u0[v] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
                     // the epilogue sees the old cell-centred field
                     const Q9<R> pm = Lay<R>::get(Pm, PN, cown);
                     const R vx = pm.v[1], vy = pm.v[2], vz = pm.v[3];
                     const R bxc = pm.v[5], byc = pm.v[6], bzc = pm.v[7];
                     q.v[5] = bxc; q.v[6] = byc; q.v[7] = bzc; q.v[8] = R(0);
                     R ax = R(0), ay = R(0), az = R(0);
-                    if (turb) force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, A.ramp, ax, ay, az);
+                    if (turb) {
+                        if constexpr (std::is_same<R, float>::value) {
+                            if (A.trig8) force_accel_f32(BS + 24 * ty, TS, tx, A.ramp, ax, ay, az);
+                            else force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, A.ramp, ax, ay, az);
+                        } else {
+                            force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, A.ramp, ax, ay, az);
+                        }
+                    }
                     finish_update(q, K, R(1), turb, ax, ay, az, A.dt);
 #pragma unroll
                     for (int v = 0; v < 5; ++v) A.o.p[v][g] = q.v[v];
@@ -350,6 +375,13 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
                     Lay<R>::put(ST + 3 * 9 * RN, RN, ir, ct_flux<1, RIEM>(Lay<R>::get(ST + 2 * 9 * RN, RN, il), Lay<R>::get(ST + 3 * 9 * RN, RN, ir), K));
                 }
             }
+        }
+        // the forcing row table of the tile's rows for plane kr, written out in the next phase
+        if constexpr (std::is_same<R, float>::value) {
+            if (turb && A.trig8 && kr >= z0 && kr < z1)
+                for (int i = tid; i < 6 * OY; i += NT)
+                    reinterpret_cast<float4*>(BS)[i] =
+                        reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + y0) * 24)[i];
         }
         if (load) {
             mbar_wait(mbar, phase, A.err, A.wait_cycles);

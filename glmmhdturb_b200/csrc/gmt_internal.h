@@ -59,6 +59,7 @@ template <class R> struct CTArgs {
     int recon, riem, emf, halfslope, do_turb;
     const R* btab;
     const R* trigx;
+    const R* trig8;        // FP32 or null: x table of 2 cos, -2 sin (force_accel_f32)
     R* scratch;            // 15 planes: lower-face EMF data and cell EMFs (12), edge EMFs (3)
     int* err;              // device flag set when a bounded wait gives up
     int use_tma;           // tmap8/tmap1 describe q: tiles clear of the box edges stage by TMA

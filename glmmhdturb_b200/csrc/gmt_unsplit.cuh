@@ -215,6 +215,9 @@ template <class R> __device__ __forceinline__ void rec_put(const UnsplitArgs<R>&
 template <class R, int RECON, int RIEM> struct UnsplitScheme {
     using Cell = Rec<R>;
     static constexpr bool kRecord = false;   // adjoint record mode (AdjRecordScheme)
+    // load the write-out's old state before the z-face solve: it pays in FP32 with HLLD, whose
+    // long solve hides the load; with HLL, and in FP64 (255 registers), it measured slower
+    static constexpr bool kEarlyOld = std::is_same<R, float>::value && RIEM == RIEM_HLLD;
     static __device__ __forceinline__ R prim_floor(const Consts<R>& K) { return K.pfl; }
     static __device__ __forceinline__ void recon(const R* PR, int PN, int PW, int c, int s0, int sm, int sp,
                                                  const Consts<R>& K, R dtdx, Cell& r) {
@@ -249,6 +252,7 @@ template <class R> struct MarchCell {
 template <class R, int RECON> struct MarchScheme {
     using Cell = MarchCell<R>;
     static constexpr bool kRecord = false;
+    static constexpr bool kEarlyOld = false;
     static __device__ __forceinline__ R prim_floor(const Consts<R>& K) { return K.smallp; }
     static __device__ __forceinline__ void recon(const R* PR, int PN, int, int c, int s0, int, int, const Consts<R>&, R,
                                                  Cell& r) {
@@ -356,8 +360,9 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     const unsigned tma_bytes = (unsigned)(9 * SN * sizeof(R));
 
     if constexpr (std::is_same<R, float>::value && !OVERHANG) {
-        if (A.trig8 && tid < 2 * OX)
-            reinterpret_cast<float4*>(TS)[tid] = reinterpret_cast<const float4*>(A.trig8 + 8 * (size_t)x0)[tid];
+        if (A.trig8)
+            for (int i = tid; i < 2 * OX; i += NT)
+                reinterpret_cast<float4*>(TS)[i] = reinterpret_cast<const float4*>(A.trig8 + 8 * (size_t)x0)[i];
     }
     // prologue: primitives of planes z0-2, z0-1, z0
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
@@ -470,20 +475,23 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
             if (!first && !last) record(4, Pz);
             if (!first) {
                 // the old state of the cell written out below, loaded before the z-face solve so that
-                // the solve hides its latency
+                // the solve hides its latency (S::kEarlyOld), else at the write-out
                 const bool wr = kr - 1 >= z0;
                 const int kf = kr - 1;
                 const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * (wr ? kf : 0));
                 Q9<R> u0;
+                if constexpr (S::kEarlyOld) {
 #pragma unroll
-                for (int v = 0; v < 9; ++v) u0.v[v] = wr ? __ldg(A.u.p[v] + g) : R(0);
+                    for (int v = 0; v < 9; ++v) u0.v[v] = wr ? __ldg(A.u.p[v] + g) : R(0);
+                }
                 Q9<R> Mz = S::template state<2, -1>(r, PR, PN, PW, cown, s0, sm, sp, K, A.iflo);
                 if (!last) record(5, Mz);
                 Q9<R> Fzhi = S::template flux<2>(pPz, Mz, K, ch, A.use_llf != 0);
                 if (wr) {
                     Q9<R> q;
 #pragma unroll
-                    for (int v = 0; v < 9; ++v) q.v[v] = u0.v[v] + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
+                    for (int v = 0; v < 9; ++v)
+                        q.v[v] = (S::kEarlyOld ? u0.v[v] : A.u.p[v][g]) + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
                     R ax = R(0), ay = R(0), az = R(0);
                     if (turb) {
                         if constexpr (std::is_same<R, float>::value) {
@@ -585,9 +593,10 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
         }
         // the forcing row table of the tile's rows for plane kr, written out in the next phase R
         if constexpr (std::is_same<R, float>::value && !OVERHANG) {
-            if (turb && A.trig8 && kr >= z0 && kr < z1 && tid < 6 * OY)
-                reinterpret_cast<float4*>(BS)[tid] =
-                    reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + y0) * 24)[tid];
+            if (turb && A.trig8 && kr >= z0 && kr < z1)
+                for (int i = tid; i < 6 * OY; i += NT)
+                    reinterpret_cast<float4*>(BS)[i] =
+                        reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + y0) * 24)[i];
         }
         if (load) {
             mbar_wait(mbar, phase, A.err, A.wait_cycles);

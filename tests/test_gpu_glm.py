@@ -60,6 +60,27 @@ def test_unsplit_tiles_vs_oracle(oracle, n, tile, recon, riem):
     assert err <= TOL_F64, (n, tile, s.kernel_info(), err)
 
 
+@pytest.mark.parametrize("n,tile", [((24, 20, 10), (8, 4, 3)), ((12, 8, 7), (4, 2, 2)), ((16, 16, 8), (4, 4, 4)),
+                                    ((96, 40, 10), (32, 8, 5)), ((96, 48, 8), (32, 16, 4))])
+def test_unsplit_fp32_tiles_with_forcing_vs_oracle(oracle, n, tile):
+    """The FP32 step stages the forcing tables of its tile in shared memory (the x table once, the
+    row table one plane ahead); tiles narrower than 6 columns have fewer threads than row-table
+    words, so the staging loops must cover them too."""
+    from glmmhdturb_b200 import Solver
+    u0 = perturbed_glm_state(oracle, n, seed=hash(n) % 1000 + 1)
+    cfg = oracle.Config(n=n, gamma=5 / 3, recon="mc", riemann="hlld", iflo=True)
+    f = oracle.OUForcing(amp=2.0, seed=5)
+    f.advance(); f.advance()
+    s = Solver(n, dtype="f32", recon="mc", riemann="hlld", gamma=5 / 3, tile=tile, turb_T=1.0)
+    s.set_modes(f.modes)
+    u = to_dev(u0, torch.float32)
+    out = torch.empty_like(u)
+    s.step(u, out, 1.5e-3, t=0.4, ch=2.0, glm_fac=0.99, do_turb=True)
+    ref = oracle.step_unsplit(cfg, u0, 1.5e-3, 2.0, 0.99, ramp=0.4, modes=f.modes)
+    err, errs = max_rel_err(out.cpu().numpy().astype(np.float64), ref)
+    assert err <= TOL_F32, (n, tile, s.kernel_info(), errs)
+
+
 def test_cfl_and_fused_cfl(oracle, golden):
     from glmmhdturb_b200 import Solver
     cfg = oracle.Config(n=G.N, gamma=G.GAMMA)
