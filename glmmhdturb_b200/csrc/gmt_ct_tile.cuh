@@ -197,7 +197,8 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
     const int nhelp = 2 * (OX + OY);
     // staging skips the helper warps, the primitive conversion the boundary-face warps (the two
     // phases' barrier tails; as in the GLM tile march)
-    const int hwarp = 32 * ((nhelp + 31) / 32), bwarp = 32 * ((OX + OY + 31) / 32);
+    const int oxp = 32 * ((OX + 31) / 32);   // boundary faces: y on [0, OX), x on [oxp, oxp + OY)
+    const int hwarp = 32 * ((nhelp + 31) / 32), bwarp = oxp + 32 * ((OY + 31) / 32);
     const int stg0 = NT - hwarp >= 32 ? hwarp : 0;
     const int nunst = NT - bwarp >= 32 ? NT - bwarp : NT;
     R* S = A.scratch;
@@ -365,14 +366,15 @@ __device__ __forceinline__ void ct_tile(const CTArgs<R>& A, int bx, int by, int 
             Lay<R>::put(ST + 1 * 9 * RN, RN, ixh, Fxh);
             Fyh = ct_flux<1, RIEM>(Lay<R>::get(ST + 2 * 9 * RN, RN, rown), Lay<R>::get(ST + 3 * 9 * RN, RN, iyh), K);
             Lay<R>::put(ST + 3 * 9 * RN, RN, iyh, Fyh);
-            for (int h = NT - 1 - tid; h < OX + OY; h += NT) {
-                if (h < OY) {
-                    const int il = 0 + RW * (h + 1), ir = 1 + RW * (h + 1);
-                    Lay<R>::put(ST + 1 * 9 * RN, RN, ir, ct_flux<0, RIEM>(Lay<R>::get(ST + 0 * 9 * RN, RN, il), Lay<R>::get(ST + 1 * 9 * RN, RN, ir), K));
-                } else {
-                    const int c = h - OY;
-                    const int il = (c + 1), ir = (c + 1) + RW;
+            for (int h = NT - 1 - tid; h < oxp + OY; h += NT) {
+                // y faces first, x faces from the next warp boundary (no warp runs both paths)
+                if (h < OX) {
+                    const int il = (h + 1), ir = (h + 1) + RW;
                     Lay<R>::put(ST + 3 * 9 * RN, RN, ir, ct_flux<1, RIEM>(Lay<R>::get(ST + 2 * 9 * RN, RN, il), Lay<R>::get(ST + 3 * 9 * RN, RN, ir), K));
+                } else if (h >= oxp) {
+                    const int f = h - oxp;
+                    const int il = 0 + RW * (f + 1), ir = 1 + RW * (f + 1);
+                    Lay<R>::put(ST + 1 * 9 * RN, RN, ir, ct_flux<0, RIEM>(Lay<R>::get(ST + 0 * 9 * RN, RN, il), Lay<R>::get(ST + 1 * 9 * RN, RN, ir), K));
                 }
             }
         }

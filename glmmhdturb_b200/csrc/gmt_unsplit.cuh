@@ -344,7 +344,8 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     // warps (phase R), boundary faces on the last ones (phase F).  The plane's staging copies skip
     // the helper warps and its primitive conversion skips the boundary-face warps, so both
     // phases' barrier tails shrink by that share (when at least one other warp remains).
-    const int hwarp = 32 * ((nhelp + 31) / 32), bwarp = 32 * ((OX + OY + 31) / 32);
+    const int oxp = 32 * ((OX + 31) / 32);   // boundary faces: y on [0, OX), x on [oxp, oxp + OY)
+    const int hwarp = 32 * ((nhelp + 31) / 32), bwarp = oxp + 32 * ((OY + 31) / 32);
     const int stg0 = NT - hwarp >= 32 ? hwarp : 0;                 // first staging thread
     const int nunst = NT - bwarp >= 32 ? NT - bwarp : NT;          // unstaging threads [0, nunst)
 
@@ -575,19 +576,21 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
             Fyh = S::template flux<1>(Lay<R>::get(ST + 2 * 9 * RN, RN, rown), Lay<R>::get(ST + 3 * 9 * RN, RN, iyh), K, ch,
                                       A.use_llf != 0);
             Lay<R>::put(ST + 3 * 9 * RN, RN, iyh, Fyh);
-            for (int h = NT - 1 - tid; h < OX + OY; h += NT) {
-                // boundary faces on the low x and low y side of the tile, taken by the last threads
-                if (h < OY) {
-                    const int il = 0 + RW * (h + 1), ir = 1 + RW * (h + 1);
-                    Q9<R> F = S::template flux<0>(Lay<R>::get(ST + 0 * 9 * RN, RN, il), Lay<R>::get(ST + 1 * 9 * RN, RN, ir), K,
-                                                  ch, A.use_llf != 0);
-                    Lay<R>::put(ST + 1 * 9 * RN, RN, ir, F);
-                } else {
-                    const int c = h - OY;
-                    const int il = (c + 1), ir = (c + 1) + RW;
+            for (int h = NT - 1 - tid; h < oxp + OY; h += NT) {
+                // boundary faces on the low x and low y side of the tile, taken by the last threads:
+                // the y faces first, the x faces from the next warp boundary, so that no warp runs
+                // both solver paths one after the other
+                if (h < OX) {
+                    const int il = (h + 1), ir = (h + 1) + RW;
                     Q9<R> F = S::template flux<1>(Lay<R>::get(ST + 2 * 9 * RN, RN, il), Lay<R>::get(ST + 3 * 9 * RN, RN, ir), K,
                                                   ch, A.use_llf != 0);
                     Lay<R>::put(ST + 3 * 9 * RN, RN, ir, F);
+                } else if (h >= oxp) {
+                    const int f = h - oxp;
+                    const int il = 0 + RW * (f + 1), ir = 1 + RW * (f + 1);
+                    Q9<R> F = S::template flux<0>(Lay<R>::get(ST + 0 * 9 * RN, RN, il), Lay<R>::get(ST + 1 * 9 * RN, RN, ir), K,
+                                                  ch, A.use_llf != 0);
+                    Lay<R>::put(ST + 1 * 9 * RN, RN, ir, F);
                 }
             }
         }
