@@ -360,10 +360,19 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     }
     const unsigned tma_bytes = (unsigned)(9 * SN * sizeof(R));
 
-    if constexpr (std::is_same<R, float>::value && !OVERHANG) {
+    if constexpr (std::is_same<R, float>::value) {
+        // two float4 per column; an overhanging tile (OVERHANG) takes its extra columns from the
+        // start of the row, as its cells do
         if (A.trig8)
-            for (int i = tid; i < 2 * OX; i += NT)
-                reinterpret_cast<float4*>(TS)[i] = reinterpret_cast<const float4*>(A.trig8 + 8 * (size_t)x0)[i];
+            for (int i = tid; i < 2 * OX; i += NT) {
+                if constexpr (OVERHANG) {
+                    int col = x0 + (i >> 1);
+                    col = col < nx ? col : col - nx;
+                    reinterpret_cast<float4*>(TS)[i] = reinterpret_cast<const float4*>(A.trig8)[2 * col + (i & 1)];
+                } else {
+                    reinterpret_cast<float4*>(TS)[i] = reinterpret_cast<const float4*>(A.trig8 + 8 * (size_t)x0)[i];
+                }
+            }
     }
     // prologue: primitives of planes z0-2, z0-1, z0
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
@@ -496,12 +505,7 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
                     R ax = R(0), ay = R(0), az = R(0);
                     if (turb) {
                         if constexpr (std::is_same<R, float>::value) {
-                            if (A.trig8) {
-                                if constexpr (OVERHANG)
-                                    force_accel_f32(A.btab + ((size_t)kf * ny + gy) * 24, A.trig8, gx, V.ramp, ax, ay, az);
-                                else
-                                    force_accel_f32(BS + 24 * ty, TS, tx, V.ramp, ax, ay, az);
-                            }
+                            if (A.trig8) force_accel_f32(BS + 24 * ty, TS, tx, V.ramp, ax, ay, az);
                             else force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
                         } else {
                             force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
@@ -595,11 +599,19 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
             }
         }
         // the forcing row table of the tile's rows for plane kr, written out in the next phase R
-        if constexpr (std::is_same<R, float>::value && !OVERHANG) {
+        if constexpr (std::is_same<R, float>::value) {
             if (turb && A.trig8 && kr >= z0 && kr < z1)
-                for (int i = tid; i < 6 * OY; i += NT)
-                    reinterpret_cast<float4*>(BS)[i] =
-                        reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + y0) * 24)[i];
+                for (int i = tid; i < 6 * OY; i += NT) {
+                    if constexpr (OVERHANG) {
+                        int row = y0 + i / 6;
+                        row = row < ny ? row : row - ny;
+                        reinterpret_cast<float4*>(BS)[i] =
+                            reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + row) * 24)[i % 6];
+                    } else {
+                        reinterpret_cast<float4*>(BS)[i] =
+                            reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + y0) * 24)[i];
+                    }
+                }
         }
         if (load) {
             mbar_wait(mbar, phase, A.err, A.wait_cycles);

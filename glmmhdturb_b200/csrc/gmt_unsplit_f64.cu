@@ -3,12 +3,29 @@
 #include "gmt_unsplit_inst.cuh"
 
 namespace gmt {
+// compile-time tiles for the production schemes (constant strides and loop bounds)
+template <int TOX, int TOY>
+static bool fixed_tile64(const UnsplitArgs<double>& A, int recon, int riem, cudaStream_t s, cudaError_t& e) {
+    if (A.ox != TOX || A.oy != TOY) return false;
+#define GMT_FIX(RC, RM) \
+    if (recon == RC && riem == RM) { e = unsplit_go<double, RC, RM, 256, 1, TOX, TOY>(A, s); return true; }
+    GMT_FIX(RECON_MC, RIEM_HLLD) GMT_FIX(RECON_MC, RIEM_HLL) GMT_FIX(RECON_PPM, RIEM_HLL)
+#undef GMT_FIX
+    return false;
+}
 cudaError_t launch_unsplit(const UnsplitArgs<double>& A, int recon, int riem, cudaStream_t s) {
     if (A.ox * A.oy > 256) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaSuccess;
+    if (fixed_tile64<32, 8>(A, recon, riem, s, e) || fixed_tile64<16, 16>(A, recon, riem, s, e)) return e;
     return unsplit_dispatch_t<double, 256, 1>(A, recon, riem, s);
 }
 cudaError_t unsplit_prepare_f64() {
     cudaError_t e = unsplit_configure_all_t<double, 256, 1>();
+#define GMT_FIX(RC, RM)                                                                          \
+    if (e == cudaSuccess) e = unsplit_configure<double, RC, RM, 256, 1, 32, 8>();                \
+    if (e == cudaSuccess) e = unsplit_configure<double, RC, RM, 256, 1, 16, 16>();
+    GMT_FIX(RECON_MC, RIEM_HLLD) GMT_FIX(RECON_MC, RIEM_HLL) GMT_FIX(RECON_PPM, RIEM_HLL)
+#undef GMT_FIX
     for (int rc = 0; e == cudaSuccess && rc < 3; ++rc)
         e = launch_ensemble((const UnsplitArgs<double>*)nullptr, nullptr, 0, nullptr, rc == 2 ? RECON_PPM : RECON_MC,
                             rc == 0 ? RIEM_HLLD : RIEM_HLL, 1, 0);
