@@ -1158,7 +1158,6 @@ struct gmt_ensemble {
     unsigned long long* cfl = nullptr;  // [2 nbox]
     double* modes = nullptr;         // [nbox][61][3][2]
     std::vector<void*> btab, trig;   // per box: row table; trig x, y, z
-    std::vector<void*> trig8;        // FP32, per box: x table of 2 cos, -2 sin (force_accel_f32)
     void* bt = nullptr;              // BoxTables<R>[nbox]
     void* args = nullptr;            // UnsplitArgs<R>[2][nbox]
     EnsItem* items = nullptr;
@@ -1193,7 +1192,7 @@ template <class R> int ens_bind(gmt_ensemble* E, void* const* u, void* const* w,
             a.do_turb = (flags & GMT_RUN_FORCING) ? 1 : 0;
             a.btab = a.do_turb ? static_cast<const R*>(E->btab[b]) : nullptr;
             a.trigx = static_cast<const R*>(E->trig[3 * b]);
-            a.trig8 = E->trig8.empty() ? nullptr : static_cast<const R*>(E->trig8[b]);
+            a.trig8 = nullptr;   // the ensemble kernel reads the generic tables (force_accel)
             a.cfl_out = E->cfl + 2 * b;
             a.err = E->err;
             a.wait_cycles = GMT_WAIT_CYCLES;
@@ -1241,7 +1240,6 @@ int gmt_ensemble_destroy(gmt_ensemble* E) {
     cudaFree(E->modes);
     for (void* x : E->btab) cudaFree(x);
     for (void* x : E->trig) cudaFree(x);
-    for (void* x : E->trig8) cudaFree(x);
     cudaFree(E->bt);
     cudaFree(E->args);
     cudaFree(E->items);
@@ -1300,10 +1298,7 @@ int gmt_ensemble_create(const gmt_params* base, int32_t nbox, const int32_t* n, 
         for (int a = 0; a < 3; ++a) A(&E->trig[3 * b + a], (size_t)8 * n[b] * E->esize);
         E->rows_max = std::max(E->rows_max, n[b] * n[b]);
     }
-    if (E->esize == 4) {
-        E->trig8.assign(nbox, nullptr);
-        for (int b = 0; b < nbox; ++b) A(&E->trig8[b], (size_t)8 * n[b] * sizeof(float));
-    }
+
     // work items: biggest boxes first, tiles of ens_tile_x x 16 columns (a box whose width is not a
     // multiple of the tile gets an overhanging last tile) x ens_lz-plane chunks (the last chunk of
     // a box may be shorter)
@@ -1342,10 +1337,7 @@ int gmt_ensemble_create(const gmt_params* base, int32_t nbox, const int32_t* n, 
                 e = cudaMemcpy(E->trig[3 * b + a], f.data(), f.size() * 4, cudaMemcpyHostToDevice);
             }
         }
-        if (E->esize == 4 && e == cudaSuccess) {
-            std::vector<float> t8 = trig8_table(t, n[b]);
-            e = cudaMemcpy(E->trig8[b], t8.data(), t8.size() * 4, cudaMemcpyHostToDevice);
-        }
+
         E->amp[b] = amp ? amp[b] : base->turb_amp;
         E->seed[b] = seeds ? seeds[b] : base->turb_seed + (uint32_t)b;
         gmt_params pb = *base;

@@ -360,19 +360,12 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
     }
     const unsigned tma_bytes = (unsigned)(9 * SN * sizeof(R));
 
-    if constexpr (std::is_same<R, float>::value) {
-        // two float4 per column; an overhanging tile (OVERHANG) takes its extra columns from the
-        // start of the row, as its cells do
+    // (the ensemble kernel, OVERHANG, keeps the tables in global memory: staged there it measured
+    // 2 % slower, its 128 registers already spilling)
+    if constexpr (std::is_same<R, float>::value && !OVERHANG) {
         if (A.trig8)
-            for (int i = tid; i < 2 * OX; i += NT) {
-                if constexpr (OVERHANG) {
-                    int col = x0 + (i >> 1);
-                    col = col < nx ? col : col - nx;
-                    reinterpret_cast<float4*>(TS)[i] = reinterpret_cast<const float4*>(A.trig8)[2 * col + (i & 1)];
-                } else {
-                    reinterpret_cast<float4*>(TS)[i] = reinterpret_cast<const float4*>(A.trig8 + 8 * (size_t)x0)[i];
-                }
-            }
+            for (int i = tid; i < 2 * OX; i += NT)
+                reinterpret_cast<float4*>(TS)[i] = reinterpret_cast<const float4*>(A.trig8 + 8 * (size_t)x0)[i];
     }
     // prologue: primitives of planes z0-2, z0-1, z0
     uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 32);
@@ -485,12 +478,13 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
             if (!first && !last) record(4, Pz);
             if (!first) {
                 // the old state of the cell written out below, loaded before the z-face solve so that
-                // the solve hides its latency (S::kEarlyOld), else at the write-out
+                // the solve hides its latency (S::kEarlyOld), else at the write-out; the ensemble
+                // kernel (OVERHANG) measured 7 % slower with the early load
                 const bool wr = kr - 1 >= z0;
                 const int kf = kr - 1;
                 const size_t g = (size_t)gx + (size_t)nx * ((size_t)gy + (size_t)ny * (wr ? kf : 0));
                 Q9<R> u0;
-                if constexpr (S::kEarlyOld) {
+                if constexpr (S::kEarlyOld && !OVERHANG) {
 #pragma unroll
                     for (int v = 0; v < 9; ++v) u0.v[v] = wr ? __ldg(A.u.p[v] + g) : R(0);
                 }
@@ -501,10 +495,10 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
                     Q9<R> q;
 #pragma unroll
                     for (int v = 0; v < 9; ++v)
-                        q.v[v] = (S::kEarlyOld ? u0.v[v] : A.u.p[v][g]) + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
+                        q.v[v] = ((S::kEarlyOld && !OVERHANG) ? u0.v[v] : A.u.p[v][g]) + dtdx * (XY.v[v] + (Fzlo.v[v] - Fzhi.v[v]));
                     R ax = R(0), ay = R(0), az = R(0);
                     if (turb) {
-                        if constexpr (std::is_same<R, float>::value) {
+                        if constexpr (std::is_same<R, float>::value && !OVERHANG) {
                             if (A.trig8) force_accel_f32(BS + 24 * ty, TS, tx, V.ramp, ax, ay, az);
                             else force_accel(A.btab + ((size_t)kf * ny + gy) * 24, A.trigx, nx, gx, V.ramp, ax, ay, az);
                         } else {
@@ -599,19 +593,11 @@ __device__ __forceinline__ void scheme_tile(const UnsplitArgs<R>& A, const StepV
             }
         }
         // the forcing row table of the tile's rows for plane kr, written out in the next phase R
-        if constexpr (std::is_same<R, float>::value) {
+        if constexpr (std::is_same<R, float>::value && !OVERHANG) {
             if (turb && A.trig8 && kr >= z0 && kr < z1)
-                for (int i = tid; i < 6 * OY; i += NT) {
-                    if constexpr (OVERHANG) {
-                        int row = y0 + i / 6;
-                        row = row < ny ? row : row - ny;
-                        reinterpret_cast<float4*>(BS)[i] =
-                            reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + row) * 24)[i % 6];
-                    } else {
-                        reinterpret_cast<float4*>(BS)[i] =
-                            reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + y0) * 24)[i];
-                    }
-                }
+                for (int i = tid; i < 6 * OY; i += NT)
+                    reinterpret_cast<float4*>(BS)[i] =
+                        reinterpret_cast<const float4*>(A.btab + ((size_t)kr * ny + y0) * 24)[i];
         }
         if (load) {
             mbar_wait(mbar, phase, A.err, A.wait_cycles);
