@@ -498,6 +498,122 @@ template <class R> __global__ void __launch_bounds__(256) ct_face_kernel(const C
     }
 }
 
+// FP32 passes B1 and B2 four cells per thread (x0 = 4k): every plane is read as one 16-byte load
+// per thread, and a neighbour one cell back (forward) in x as the same quad shifted by one cell,
+// its outside value read separately (from the other end of the row at the periodic boundary).
+// Requires nx % 4 == 0 and 16-byte aligned planes; the per-cell arithmetic is the scalar passes'.
+struct CTQuad {
+    const float* S;
+    size_t n;
+    int x, nx;
+    __device__ __forceinline__ float4 at(int plane, size_t base) const {
+        return __ldg(reinterpret_cast<const float4*>(S + (size_t)plane * n + base));
+    }
+    // cells base-1 .. base+2 (base is the first cell of a quad at column x of its row)
+    __device__ __forceinline__ float4 back(int plane, size_t base) const {
+        const float4 q = at(plane, base);
+        const float w = __ldg(S + (size_t)plane * n + (x == 0 ? base + nx - 1 : base - 1));
+        return make_float4(w, q.x, q.y, q.z);
+    }
+};
+__device__ __forceinline__ float q4(const float4& v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); }
+
+template <bool CONTACT> __global__ void __launch_bounds__(256) ct_edge_kernel4(const CTArgs<float> A) {
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const size_t n = (size_t)nx * ny * nz, nq = n / 4;
+    float* W = A.scratch;
+    for (size_t qd = (size_t)blockIdx.x * blockDim.x + threadIdx.x; qd < nq; qd += (size_t)gridDim.x * blockDim.x) {
+        const size_t c = 4 * qd;
+        int x, y, z;
+        cell_coords(c, nx, ny, n, x, y, z);
+        const CTQuad Q{A.scratch, n, x, nx};
+        const size_t ym = (size_t)x + (size_t)nx * (wrap1(y - 1, ny) + (size_t)ny * z);
+        const size_t zm = (size_t)x + (size_t)nx * (y + (size_t)ny * wrap1(z - 1, nz));
+        const size_t yzm = (size_t)x + (size_t)nx * (wrap1(y - 1, ny) + (size_t)ny * wrap1(z - 1, nz));
+        // per edge e as in ct_edge_kernel: EaN, EaS, EbE, EbW, then e00, e10, e01, e11, maN, maS, mbE, mbW
+        float4 v[3][CONTACT ? 12 : 4];
+        // e = 0: (A,B) = (y,z), c10 = y-1, c01 = z-1
+        v[0][0] = Q.at(CS_EXY, c); v[0][1] = Q.at(CS_EXY, zm); v[0][2] = Q.at(CS_EXZ, c); v[0][3] = Q.at(CS_EXZ, ym);
+        // e = 1: (A,B) = (z,x), c10 = z-1, c01 = x-1
+        v[1][0] = Q.at(CS_EYZ, c); v[1][1] = Q.back(CS_EYZ, c); v[1][2] = Q.at(CS_EYX, c); v[1][3] = Q.at(CS_EYX, zm);
+        // e = 2: (A,B) = (x,y), c10 = x-1, c01 = y-1
+        v[2][0] = Q.at(CS_EZX, c); v[2][1] = Q.at(CS_EZX, ym); v[2][2] = Q.at(CS_EZY, c); v[2][3] = Q.back(CS_EZY, c);
+        if constexpr (CONTACT) {
+            v[0][4] = Q.at(CS_ECX, c); v[0][5] = Q.at(CS_ECX, ym); v[0][6] = Q.at(CS_ECX, zm); v[0][7] = Q.at(CS_ECX, yzm);
+            v[0][8] = Q.at(CS_MY, c); v[0][9] = Q.at(CS_MY, zm); v[0][10] = Q.at(CS_MZ, c); v[0][11] = Q.at(CS_MZ, ym);
+            v[1][4] = Q.at(CS_ECY, c); v[1][5] = Q.at(CS_ECY, zm); v[1][6] = Q.back(CS_ECY, c); v[1][7] = Q.back(CS_ECY, zm);
+            v[1][8] = Q.at(CS_MZ, c); v[1][9] = Q.back(CS_MZ, c); v[1][10] = Q.at(CS_MX, c); v[1][11] = Q.at(CS_MX, zm);
+            v[2][4] = Q.at(CS_ECZ, c); v[2][5] = Q.back(CS_ECZ, c); v[2][6] = Q.at(CS_ECZ, ym); v[2][7] = Q.back(CS_ECZ, ym);
+            v[2][8] = Q.at(CS_MX, c); v[2][9] = Q.at(CS_MX, ym); v[2][10] = Q.at(CS_MY, c); v[2][11] = Q.back(CS_MY, c);
+        }
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            float out[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float EaN = q4(v[e][0], j), EaS = q4(v[e][1], j), EbE = q4(v[e][2], j), EbW = q4(v[e][3], j);
+                float E = 0.25f * (EbE + EbW + EaN + EaS);
+                if constexpr (CONTACT) {
+                    const float e00 = q4(v[e][4], j), e10 = q4(v[e][5], j), e01 = q4(v[e][6], j), e11 = q4(v[e][7], j);
+                    const float dN = ct_upwind(q4(v[e][8], j), e10 - EbW, e00 - EbE);
+                    const float dS = ct_upwind(q4(v[e][9], j), EbW - e11, EbE - e01);
+                    const float dE = ct_upwind(q4(v[e][10], j), e01 - EaS, e00 - EaN);
+                    const float dW = ct_upwind(q4(v[e][11], j), EaS - e11, EaN - e10);
+                    E = E + 0.25f * (dS - dN) + 0.25f * (dW - dE);
+                }
+                out[j] = E;
+            }
+            *reinterpret_cast<float4*>(W + (size_t)(CS_EDX + e) * n + c) = make_float4(out[0], out[1], out[2], out[3]);
+        }
+    }
+}
+
+template <class R> __global__ void __launch_bounds__(256) ct_face_kernel4(const CTArgs<R> A) {
+    static_assert(std::is_same<R, float>::value, "the 4-wide CT passes are FP32");
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const size_t n = (size_t)nx * ny * nz, nq = n / 4;
+    const float* ex = A.scratch + CS_EDX * n;
+    const float* ey = A.scratch + CS_EDY * n;
+    const float* ez = A.scratch + CS_EDZ * n;
+    const float dtdx = A.dtdx;
+    for (size_t qd = (size_t)blockIdx.x * blockDim.x + threadIdx.x; qd < nq; qd += (size_t)gridDim.x * blockDim.x) {
+        const size_t c = 4 * qd;
+        int x, y, z;
+        cell_coords(c, nx, ny, n, x, y, z);
+        const size_t cyp = (size_t)x + (size_t)nx * (wrap1(y + 1, ny) + (size_t)ny * z);
+        const size_t czp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrap1(z + 1, nz));
+        const size_t cxn = x + 4 == nx ? c + 4 - nx : c + 4;   // first cell of the next quad of the row
+        auto ld = [](const float* p, size_t i) { return __ldg(reinterpret_cast<const float4*>(p + i)); };
+        // every load before the first store (the outputs may share an allocation with the inputs)
+        const float4 exc = ld(ex, c), eyc = ld(ey, c), ezc = ld(ez, c);
+        const float4 ezy = ld(ez, cyp), eyz = ld(ey, czp), exz = ld(ex, czp), exy = ld(ex, cyp);
+        const float4 ezq = ezc, eyq = eyc;
+        const float ezn = __ldg(ez + cxn), eyn = __ldg(ey + cxn);
+        const float4 ezx = make_float4(ezq.y, ezq.z, ezq.w, ezn), eyx = make_float4(eyq.y, eyq.z, eyq.w, eyn);
+        const float4 b5 = ld(A.q.p[5], c), b6 = ld(A.q.p[6], c), b7 = ld(A.q.p[7], c);
+        float o5[4], o6[4], o7[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            o5[j] = q4(b5, j) - dtdx * ((q4(ezy, j) - q4(ezc, j)) - (q4(eyz, j) - q4(eyc, j)));
+            o6[j] = q4(b6, j) - dtdx * ((q4(exz, j) - q4(exc, j)) - (q4(ezx, j) - q4(ezc, j)));
+            o7[j] = q4(b7, j) - dtdx * ((q4(eyx, j) - q4(eyc, j)) - (q4(exy, j) - q4(exc, j)));
+        }
+        *reinterpret_cast<float4*>(A.o.p[5] + c) = make_float4(o5[0], o5[1], o5[2], o5[3]);
+        *reinterpret_cast<float4*>(A.o.p[6] + c) = make_float4(o6[0], o6[1], o6[2], o6[3]);
+        *reinterpret_cast<float4*>(A.o.p[7] + c) = make_float4(o7[0], o7[1], o7[2], o7[3]);
+    }
+}
+
+// the 4-wide passes apply: FP32, nx a multiple of 4, every plane they touch 16-byte aligned
+template <class R> inline bool ct_quad_ok(const CTArgs<R>& A) {
+    if (sizeof(R) != 4 || A.nx % 4 != 0) return false;
+    auto al = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+    if (!al(A.scratch) || ((size_t)A.nx * A.ny * A.nz) % 4 != 0) return false;
+    for (int v = 5; v < 8; ++v)
+        if (!al(A.q.p[v]) || !al(A.o.p[v])) return false;
+    return true;
+}
+
 // launch: pass A (tile kernel), then B1 and B2; nt <= 0 in A configures the kernel only
 template <class R, int RECON, int RIEM, int MAXT, int MINB, int TOX = 0, int TOY = 0>
 static cudaError_t ct_go(const CTArgs<R>& A, cudaStream_t s, bool configure_only) {
@@ -513,6 +629,15 @@ static cudaError_t ct_go(const CTArgs<R>& A, cudaStream_t s, bool configure_only
     dim3 grid(A.nx / A.ox, A.ny / A.oy, (A.nz + A.lz - 1) / A.lz);
     k<<<grid, nt, ct_tile_smem_bytes<R>(A.ox, A.oy), s>>>(A);
     const size_t n = (size_t)A.nx * A.ny * A.nz;
+    if constexpr (std::is_same<R, float>::value) {
+        if (ct_quad_ok(A)) {
+            const int nb4 = (int)std::min<size_t>((n / 4 + 255) / 256, (size_t)148 * 16);
+            if (A.emf == 1) ct_edge_kernel4<true><<<nb4, 256, 0, s>>>(A);
+            else ct_edge_kernel4<false><<<nb4, 256, 0, s>>>(A);
+            ct_face_kernel4<R><<<nb4, 256, 0, s>>>(A);
+            return cudaGetLastError();
+        }
+    }
     const int nb = (int)std::min<size_t>((n + 255) / 256, (size_t)148 * 16);
     if (A.emf == 1) ct_edge_kernel<R, true><<<nb, 256, 0, s>>>(A);
     else ct_edge_kernel<R, false><<<nb, 256, 0, s>>>(A);
