@@ -518,7 +518,9 @@ struct CTQuad {
 };
 __device__ __forceinline__ float q4(const float4& v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); }
 
-template <bool CONTACT> __global__ void __launch_bounds__(256) ct_edge_kernel4(const CTArgs<float> A) {
+// three blocks per SM (at most 85 registers, a 40-byte spill): 2.8 % faster for the whole CT step than
+// two blocks at 92 registers, the pass being bound by loads in flight
+template <bool CONTACT> __global__ void __launch_bounds__(256, 3) ct_edge_kernel4(const CTArgs<float> A) {
     const int nx = A.nx, ny = A.ny, nz = A.nz;
     const size_t n = (size_t)nx * ny * nz, nq = n / 4;
     float* W = A.scratch;

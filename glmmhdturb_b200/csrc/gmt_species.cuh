@@ -93,8 +93,145 @@ __global__ void __launch_bounds__(128) species_kernel(const MarchArgs<R> A, cons
     }
 }
 
+// FP32 species pass, four cells x0..x0+3 (x0 = 4k) per thread: every plane is read as 16-byte
+// quads (the x stencil from the quads at x0-4, x0, x0+4 of the row, periodic), the five x faces
+// x0-1/2 .. x0+7/2 are each solved once, and the result is stored as one quad per species.  Same
+// per-face and per-cell arithmetic as species_kernel.  Requires nx % 4 == 0, nx >= 8 and 16-byte
+// aligned planes.
+__device__ __forceinline__ float sq4(const float4& v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); }
+
+template <int NSP> __global__ void __launch_bounds__(128) species_kernel4(const MarchArgs<float> A, const float* __restrict__ fmass) {
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const size_t n = (size_t)nx * ny * nz, nq = n / 4;
+    const float h = 0.5f * A.dtdx;
+    const bool ppm = A.ppm != 0;
+    auto ld = [](const float* p, size_t i) { return __ldg(reinterpret_cast<const float4*>(p + i)); };
+    auto wrap2 = [](int i, int m) {   // as species_kernel: boxes narrower than the stencil wrap twice
+        i = i < 0 ? i + m : (i >= m ? i - m : i);
+        return i < 0 ? i + m : (i >= m ? i - m : i);
+    };
+    for (size_t qd = (size_t)blockIdx.x * blockDim.x + threadIdx.x; qd < nq; qd += (size_t)gridDim.x * blockDim.x) {
+        const size_t c = 4 * qd;
+        int x, y, z;
+        cell_coords(c, nx, ny, n, x, y, z);
+        float divs[NSP][4];
+#pragma unroll
+        for (int sp = 0; sp < NSP; ++sp)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) divs[sp][j] = 0.0f;
+        // ---- x: the 8 cells x0-2 .. x0+5 from three quads
+        {
+            const size_t cm = x == 0 ? c + nx - 4 : c - 4, cp = x + 4 == nx ? c + 4 - nx : c + 4;
+            float rho[8], un[6];
+            {
+                const float4 a = ld(A.u.p[0], cm), b = ld(A.u.p[0], c), d = ld(A.u.p[0], cp);
+                const float r[8] = {a.z, a.w, b.x, b.y, b.z, b.w, d.x, d.y};
+#pragma unroll
+                for (int k = 0; k < 8; ++k) rho[k] = rmax(r[k], A.K.smallr);
+            }
+            {
+                const float4 a = ld(A.u.p[1], cm), b = ld(A.u.p[1], c), d = ld(A.u.p[1], cp);
+                const float m[6] = {a.w, b.x, b.y, b.z, b.w, d.x};   // cells x0-1 .. x0+4
+#pragma unroll
+                for (int k = 0; k < 6; ++k) un[k] = m[k] * (1.0f / rho[k + 1]);
+            }
+            const float4 f0 = ld(fmass, c), f1 = ld(fmass, cp);
+            const float F[5] = {f0.x, f0.y, f0.z, f0.w, f1.x};   // faces x0-1/2 .. x0+7/2
+#pragma unroll
+            for (int sp = 0; sp < NSP; ++sp) {
+                {
+                    const float4 a = ld(A.su[sp], cm), b = ld(A.su[sp], c), d = ld(A.su[sp], cp);
+                    const float v[8] = {a.z, a.w, b.x, b.y, b.z, b.w, d.x, d.y};
+                    float X[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) X[k] = v[k] / rho[k];
+                    float f[5];
+#pragma unroll
+                    for (int k = 0; k < 5; ++k)   // face x0+k-1/2: cells x0+k-2 .. x0+k+1 = X[k..k+3]
+                        f[k] = species_face(X[k], X[k + 1], X[k + 2], X[k + 3], un[k], un[k + 1], h, F[k], ppm);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) divs[sp][j] = divs[sp][j] + (f[j + 1] - f[j]);
+                }
+            }
+        }
+        // ---- y and z: five rows (planes) of quads
+#pragma unroll
+        for (int D = 1; D < 3; ++D) {
+            const int cc = D == 1 ? y : z, m = D == 1 ? ny : nz;
+            const size_t st = D == 1 ? (size_t)nx : (size_t)nx * ny;
+            size_t at[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) at[k] = c + (size_t)((long long)(wrap2(cc + k - 2, m) - cc) * (long long)st);
+            float4 rho[5], un[3];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                const float4 r = ld(A.u.p[0], at[k]);
+                rho[k] = make_float4(rmax(r.x, A.K.smallr), rmax(r.y, A.K.smallr), rmax(r.z, A.K.smallr), rmax(r.w, A.K.smallr));
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float4 u = ld(A.u.p[1 + D], at[k + 1]);
+                un[k] = make_float4(u.x * (1.0f / rho[k + 1].x), u.y * (1.0f / rho[k + 1].y), u.z * (1.0f / rho[k + 1].z),
+                                    u.w * (1.0f / rho[k + 1].w));
+            }
+            const float4 Fm = ld(fmass + (size_t)D * n, c), Fp = ld(fmass + (size_t)D * n, at[3]);
+#pragma unroll
+            for (int sp = 0; sp < NSP; ++sp) {
+                {
+                    float4 X[5];
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) {
+                        const float4 v = ld(A.su[sp], at[k]);
+                        X[k] = make_float4(v.x / rho[k].x, v.y / rho[k].y, v.z / rho[k].z, v.w / rho[k].w);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float fm = species_face(sq4(X[0], j), sq4(X[1], j), sq4(X[2], j), sq4(X[3], j), sq4(un[0], j),
+                                                      sq4(un[1], j), h, sq4(Fm, j), ppm);
+                        const float fp = species_face(sq4(X[1], j), sq4(X[2], j), sq4(X[3], j), sq4(X[4], j), sq4(un[1], j),
+                                                      sq4(un[2], j), h, sq4(Fp, j), ppm);
+                        divs[sp][j] = divs[sp][j] + (fp - fm);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int sp = 0; sp < NSP; ++sp) {
+            {
+                const float4 u0 = ld(A.su[sp], c);
+                *reinterpret_cast<float4*>(A.so[sp] + c) =
+                    make_float4(u0.x - A.dtdx * divs[sp][0], u0.y - A.dtdx * divs[sp][1], u0.z - A.dtdx * divs[sp][2],
+                                u0.w - A.dtdx * divs[sp][3]);
+            }
+        }
+    }
+}
+
+// the 4-wide pass applies: FP32, nx a multiple of 4 and at least 8, every plane 16-byte aligned
+inline bool species_quad_ok(const MarchArgs<float>& A, const float* fmass) {
+    if (A.nx % 4 != 0 || A.nx < 8) return false;
+    auto al = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+    if (!al(fmass) || !al(A.u.p[0]) || !al(A.u.p[1]) || !al(A.u.p[2]) || !al(A.u.p[3])) return false;
+    for (int sp = 0; sp < A.nsp; ++sp)
+        if (!al(A.su[sp]) || !al(A.so[sp])) return false;
+    return true;
+}
+
 template <class R> static cudaError_t species_go(const MarchArgs<R>& A, const R* fmass, cudaStream_t s) {
     size_t n = (size_t)A.nx * A.ny * A.nz;
+    if constexpr (std::is_same<R, float>::value) {
+        if (species_quad_ok(A, fmass)) {
+            const int nb4 = (int)std::min<size_t>((n / 4 + 127) / 128, (size_t)148 * 64);
+            switch (A.nsp) {   // the species count is a template parameter (registers per species)
+                case 1: species_kernel4<1><<<nb4, 128, 0, s>>>(A, fmass); break;
+                case 2: species_kernel4<2><<<nb4, 128, 0, s>>>(A, fmass); break;
+                case 3: species_kernel4<3><<<nb4, 128, 0, s>>>(A, fmass); break;
+                case 4: species_kernel4<4><<<nb4, 128, 0, s>>>(A, fmass); break;
+                default: species_kernel<R><<<(int)std::min<size_t>((n + 127) / 128, (size_t)148 * 64), 128, 0, s>>>(A, fmass);
+            }
+            return cudaGetLastError();
+        }
+    }
     int nb = (int)std::min<size_t>((n + 127) / 128, (size_t)148 * 64);
     species_kernel<R><<<nb, 128, 0, s>>>(A, fmass);
     return cudaGetLastError();
