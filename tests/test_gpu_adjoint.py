@@ -99,7 +99,7 @@ def _scaled(sched, f):
 
 
 def _forced_base(n, seed=0, sigma=1e-3, dtype="f64"):
-    """configs[0]-type state: uniform (rho 1, p 0.6, B (0.775,0,0)) plus a seeded Gaussian
+    """The 64^3 parity run's kind of state: uniform (rho 1, p 0.6, B (0.775,0,0)) plus a seeded Gaussian
     perturbation (sigma) of v and B; returns (solver, u0, direction of the perturbation)."""
     from glmmhdturb_b200 import adjoint as AD
     s = _solver(n, dtype=dtype)
@@ -226,7 +226,7 @@ def test_adjoint_rejects_ppm_and_aliasing():
         s2.adjoint_step(u2, g2, g2, 1e-3, ch=1.0, glm_fac=1.0)
 
 
-def test_configs3_64cube_50_steps_fp64():
+def test_adjoint_64cube_50_steps_fp64():
     """The differentiable-run configuration: 64^3, 50 forced steps with dt frozen, loss = KE shell
     power 4 <= |k| <= 8 at the last step, checkpoints every 10; gradients with respect to the OU
     amplitude and the seeded (sigma = 1e-3) initial velocity/B perturbation vs central differences."""
@@ -244,14 +244,14 @@ def test_configs3_64cube_50_steps_fp64():
     eu = 1e-6
     fd_u = (loss_of(u0 + eu * d, sched) - loss_of(u0 - eu * d, sched)) / (2 * eu)
     ad_u = AD.dot(r["grad_u0"], d)
-    print("configs[3] loss %.6e  dL/damp adjoint %.10e fd %.10e  dL/dalpha adjoint %.10e fd %.10e"
+    print("64^3 x 50 adjoint: loss %.6e  dL/damp adjoint %.10e fd %.10e  dL/dalpha adjoint %.10e fd %.10e"
           % (r["loss"], r["grad_amp"], fd_amp, ad_u, fd_u))
     assert _rel(r["grad_amp"], fd_amp) <= FD_TOL
     assert _rel(ad_u, fd_u) <= FD_TOL
 
 
-def test_configs3_forward_mode_directions_fp64(oracle):
-    """configs[3] gradient against the oracle's forward-mode directional derivatives over all 50
+def test_adjoint_64cube_forward_mode_directions_fp64(oracle):
+    """The 64^3 x 50-step gradient against the oracle's forward-mode directional derivatives over all 50
     steps along 7 random state directions (all nine fields) and the forcing amplitude."""
     from glmmhdturb_b200 import adjoint as AD
     n, nsteps = 64, 50
@@ -282,7 +282,7 @@ def test_configs3_forward_mode_directions_fp64(oracle):
     assert _rel(fwd_amp, r["grad_amp"]) <= 1e-8, (fwd_amp, r["grad_amp"])
 
 
-def test_configs4_adjoint_128cube_200_steps_in_40gb():
+def test_adjoint_128cube_200_steps_in_40gb():
     """The large adjoint: 128^3 FP32, 200 forced steps, checkpoint interval from a 40 GB budget
     with recomputation; finite gradients, device memory within the budget."""
     import time
@@ -298,7 +298,7 @@ def test_configs4_adjoint_128cube_200_steps_in_40gb():
     torch.cuda.synchronize()
     elapsed = time.perf_counter() - t0
     peak = torch.cuda.max_memory_allocated() + AD.adjoint_scratch_bytes(s)
-    print(f"configs[4] adjoint 128^3 x {nsteps}: K={K}, {elapsed:.2f} s forward+backward, "
+    print(f"adjoint 128^3 x {nsteps}: K={K}, {elapsed:.2f} s forward+backward, "
           f"peak {peak / 2**30:.2f} GB (torch tensors + adjoint scratch), dL/damp {r['grad_amp']:.4e}")
     assert math.isfinite(r["grad_amp"]) and bool(torch.isfinite(r["grad_u0"]).all())
     assert peak <= budget

@@ -77,7 +77,7 @@ def test_ct_fullsize_divergence_roundoff():
     assert d0 < 1e-3 and d1 < 1e-3, (d0, d1)
 
 
-def test_configs4_1024cube_forward_20_steps():
+def test_forward_1024cube_fp32_20_steps():
     """The large-scale forward configuration: 1024^3 FP32, PLM-MC + HLLD + GLM with forcing, from the
     uniform state (rho 1, p 0.6, B0 = (0.775, 0, 0)) with the forcing amplitude 4x the Mach-1
     calibration (stationary rms Mach ~2: v^2 grows with the amplitude), seed 2; 20 steps, two
@@ -113,7 +113,7 @@ def test_configs4_1024cube_forward_20_steps():
     ms = e0.elapsed_time(e1) / 20
     d = s.diagnostics(u)
     rate = n ** 3 / (ms * 1e-3)
-    print(json.dumps({"configs4_forward_1024": {"ms_per_step": ms, "gzone_per_s": rate / 1e9, "t": t,
+    print(json.dumps({"forward_1024cube_fp32": {"ms_per_step": ms, "gzone_per_s": rate / 1e9, "t": t,
                                                 "vrms": d["vrms"], "mass_rel_change": d["mass"] / mass0 - 1}}))
     assert d["finite"] and abs(d["mass"] / mass0 - 1.0) <= 1e-5
     assert rate >= 9e9, ms

@@ -136,21 +136,21 @@ def test_nonfinite_state_reports_error(golden):
 
 
 # ---------------------------------------------------------------------------------------------
-# 64^3 FP64, rho=1, v=0, p=0.6, B0=(0.775,0,0), psi=0, gamma=5/3, PLM-MC + Hancock +
+# the 64^3 parity configuration: FP64, rho=1, v=0, p=0.6, B0=(0.775,0,0), psi=0, gamma=5/3, PLM-MC + Hancock +
 # HLLD, ch = global max fast signal speed, c_p^2/c_h = 0.18, OU modes 1<=|k|<=3, tau=0.5, seed 0,
 # CFL 0.3, 100 steps; all 9 fields against the oracle.
 # ---------------------------------------------------------------------------------------------
 # forcing amplitude (stationary rms acceleration) calibrated so that the rms Mach number reaches 1 at
 # t = 2 tau (tests/golden/calibrate_amp.py, bisection with the FP64 oracle at 64^3)
-CFG0_AMP = G.calibrated_amp()
+PARITY64_AMP = G.calibrated_amp()
 
 
 @pytest.fixture(scope="module")
-def config0_oracle(oracle):
+def parity64_oracle(oracle):
     n = (64, 64, 64)
     cfg = oracle.Config(n=n, gamma=5 / 3, recon="mc", riemann="hlld", iflo=True)
     u = oracle.ic_uniform(cfg, 1.0, 0.6, (0.775, 0.0, 0.0))
-    f = oracle.OUForcing(amp=CFG0_AMP, T=0.5, ndt=100, seed=0)
+    f = oracle.OUForcing(amp=PARITY64_AMP, T=0.5, ndt=100, seed=0)
     f.advance()
     t = 0.0
     traj = []
@@ -167,11 +167,11 @@ def config0_oracle(oracle):
     return u, traj
 
 
-def test_config0_fp64_100_steps(config0_oracle):
+def test_parity64_fp64_100_steps(parity64_oracle):
     from glmmhdturb_b200 import Solver
-    ref, traj = config0_oracle
+    ref, traj = parity64_oracle
     n = (64, 64, 64)
-    s = Solver(n, dtype="f64", gamma=5 / 3, turb_T=0.5, turb_amp=CFG0_AMP, turb_seed=0, courant=0.3)
+    s = Solver(n, dtype="f64", gamma=5 / 3, turb_T=0.5, turb_amp=PARITY64_AMP, turb_seed=0, courant=0.3)
     u = s.alloc()
     s.ic_uniform(u, 1.0, 0.6, (0.775, 0.0, 0.0))
     w = torch.empty_like(u)
@@ -184,16 +184,16 @@ def test_config0_fp64_100_steps(config0_oracle):
         s.step(u, w, dt, t=t, ch=ch, glm_fac=fac, do_turb=True)
         u, w = w, u
     err, errs = max_rel_err(u.cpu().numpy(), ref)
-    print("configs[0] FP64 per-field max rel err after 100 steps:", ["%.2e" % e for e in errs])
+    print("64^3 parity run, FP64 per-field max rel err after 100 steps:", ["%.2e" % e for e in errs])
     assert err <= TOL_F64, errs
 
 
-def test_config0_fp32_100_steps_error(config0_oracle):
+def test_parity64_fp32_100_steps_error(parity64_oracle):
     """FP32 build against the FP64 oracle after 100 steps (stated, bounded)."""
     from glmmhdturb_b200 import Solver
-    ref, traj = config0_oracle
+    ref, traj = parity64_oracle
     n = (64, 64, 64)
-    s = Solver(n, dtype="f32", gamma=5 / 3, turb_T=0.5, turb_amp=CFG0_AMP, turb_seed=0, courant=0.3)
+    s = Solver(n, dtype="f32", gamma=5 / 3, turb_T=0.5, turb_amp=PARITY64_AMP, turb_seed=0, courant=0.3)
     u = s.alloc()
     s.ic_uniform(u, 1.0, 0.6, (0.775, 0.0, 0.0))
     w = torch.empty_like(u)
@@ -204,8 +204,8 @@ def test_config0_fp32_100_steps_error(config0_oracle):
     got = u.cpu().numpy().astype(np.float64)
     err, errs = max_rel_err(got, ref)
     rel2 = [float(np.linalg.norm(got[v] - ref[v]) / max(np.linalg.norm(ref[v]), 1e-300)) for v in range(9)]
-    print("configs[0] FP32 per-field max rel err after 100 steps:", ["%.2e" % e for e in errs])
-    print("configs[0] FP32 per-field relL2 after 100 steps:", ["%.2e" % e for e in rel2])
+    print("64^3 parity run, FP32 per-field max rel err after 100 steps:", ["%.2e" % e for e in errs])
+    print("64^3 parity run, FP32 per-field relL2 after 100 steps:", ["%.2e" % e for e in rel2])
     # rho, momentum, E, B: FP32 round-off of O(0.01) perturbations on an O(1) background; psi is a
     # small cleaning field sourced by round-off-level div B, so its field-scale error is larger.
     # Measured (calibrated amplitude): field-scale max 1.44e-5 (By), relL2 8.6e-6; psi 3.4e-3 / 4.8e-3
