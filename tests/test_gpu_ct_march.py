@@ -291,3 +291,56 @@ def test_fp32_production_tile_vs_oracle(oracle, scheme, recon, riem):
     np.testing.assert_array_equal(outs[((32, 16, 0), False)], outs[((32, 16, 0), True)])
     err, errs = max_rel_err(outs[((32, 16, 0), False)], outs[((16, 16, 0), False)].astype(np.float64))
     assert max(errs[:8]) <= 1e-5, errs
+
+
+def _offset_copy(t):
+    """The values of t in a buffer one element further on, so that every plane starts 4 bytes off a
+    16-byte boundary: the library then stages by cp.async and takes its one-cell-per-thread passes."""
+    big = torch.empty(t.numel() + 4, dtype=t.dtype, device=t.device)
+    v = big[1:1 + t.numel()].view(t.shape)
+    v.copy_(t)
+    assert v.data_ptr() % 16 != 0
+    return v
+
+
+def test_fp32_quad_passes_match_one_cell_passes():
+    """In FP32 the CT edge and face passes and the species pass run four cells per thread when every
+    plane is 16-byte aligned (and nx is a multiple of 4); misaligned planes take the one-cell
+    passes.  CT: bit-identical.  Species: equal up to the last bit of the fraction divisions."""
+    from glmmhdturb_b200 import Solver
+    n = (64, 32, 16)
+    s = Solver(n, dtype="f32", scheme="ct", recon="mc", riemann="hlld", emf="contact", gamma=5 / 3, turb_amp=2.0,
+               turb_T=0.5)
+    q = s.alloc()
+    s.ic_turbulent(q, mach=1.0, seed=3)
+    s.forcing_advance()
+    a = torch.empty_like(q)
+    s.step(q, a, 1e-4, t=0.2, do_turb=True)
+    qm = _offset_copy(q)
+    am = _offset_copy(torch.zeros_like(q))
+    s.step(qm, am, 1e-4, t=0.2, do_turb=True)
+    torch.cuda.synchronize()
+    assert torch.equal(a, am)
+
+    nsp = 2
+    m = Solver(n, dtype="f32", scheme="march1d", recon="mc", riemann="hll", gamma=5 / 3, nsp=nsp)
+    u = m.alloc()
+    g = Solver(n, dtype="f32", gamma=5 / 3)
+    u9 = g.alloc()
+    g.ic_turbulent(u9, 1.0, 0.6, (0.775, 0.0, 0.0), mach=1.0, db=0.1, seed=4)
+    u.zero_()
+    u[:9] = u9
+    x = torch.arange(n[0], device="cuda", dtype=torch.float32)
+    u[9] = u9[0] * (0.3 + 0.2 * torch.sin(0.4 * x))
+    u[10] = u9[0] * (0.7 - 0.2 * torch.sin(0.4 * x))
+    cm, sm = m.cfl(u)
+    dt = 0.3 * m.dx / cm
+    w = torch.empty_like(u)
+    m.step(u, w, dt, ch=sm, glm_fac=0.99)
+    um = _offset_copy(u)
+    wm = _offset_copy(torch.zeros_like(u))
+    m.step(um, wm, dt, ch=sm, glm_fac=0.99)
+    torch.cuda.synchronize()
+    assert torch.equal(w[:9], wm[:9])
+    d = (w[9:] - wm[9:]).abs().max().item()
+    assert d <= 1e-6 * w[9:].abs().max().item(), d
