@@ -149,9 +149,75 @@ __global__ void __launch_bounds__(256) diag_final(const double* partials, int nb
         for (int k = 0; k < NDIAG; ++k) out[k] = sh[k];
 }
 
+// FP32 diagnostics four cells x0..x0+3 (x0 = 4k) per thread: 16-byte loads of every plane, the
+// x neighbours of Bx from the quad plus the cells either side of it (periodic); each cell's
+// contributions are the scalar kernel's, accumulated in FP64 in cell order within the quad.
+__global__ void __launch_bounds__(256) diag_kernel4(const CPlanes<float> u, int nx, int ny, int nz, double dx,
+                                                    double smallr, double* partials) {
+    __shared__ double sh[256 * NDIAG];
+    double acc[NDIAG] = {0, 0, 0, 0, 0, 0, 1e300, 0};
+    const size_t n = (size_t)nx * ny * nz, nq = n / 4;
+    auto ld = [](const float* p, size_t i) { return __ldg(reinterpret_cast<const float4*>(p + i)); };
+    auto el = [](const float4& v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); };
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t c = 4 * q;
+        int x, y, z;
+        cell_coords(c, nx, ny, n, x, y, z);
+        const size_t cyp = (size_t)x + (size_t)nx * (wrap1(y + 1, ny) + (size_t)ny * z);
+        const size_t cym = (size_t)x + (size_t)nx * (wrap1(y - 1, ny) + (size_t)ny * z);
+        const size_t czp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrap1(z + 1, nz));
+        const size_t czm = (size_t)x + (size_t)nx * (y + (size_t)ny * wrap1(z - 1, nz));
+        float4 v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = ld(u.p[k], c);
+        const float4 byp = ld(u.p[6], cyp), bym = ld(u.p[6], cym), bzp = ld(u.p[7], czp), bzm = ld(u.p[7], czm);
+        const float bxl = __ldg(u.p[5] + (x == 0 ? c + nx - 1 : c - 1));       // cell x0-1
+        const float bxr = __ldg(u.p[5] + (x + 4 == nx ? c + 4 - nx : c + 4));  // cell x0+4
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double rho = (double)el(v[0], j), mx = (double)el(v[1], j), my = (double)el(v[2], j),
+                         mz = (double)el(v[3], j), ps = (double)el(v[8], j);
+            acc[0] += rho;
+            acc[1] += (mx * mx + my * my + mz * mz) / fmax(rho, smallr);
+            acc[2] += (double)el(v[4], j);
+            acc[3] += ps * ps;
+            const double bxp = j < 3 ? el(v[5], j + 1) : bxr, bxm = j > 0 ? el(v[5], j - 1) : bxl;
+            const double byp_ = el(byp, j), bym_ = el(bym, j), bzp_ = el(bzp, j), bzm_ = el(bzm, j);
+            const double db = fabs((bxp - bxm) + (byp_ - bym_) + (bzp_ - bzm_)) / (2.0 * dx);
+            acc[4] += db * db;
+            acc[5] = fmax(acc[5], db);
+            acc[6] = fmin(acc[6], rho);
+            bool fin = true;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) fin = fin && isfinite((double)el(v[k], j));
+            acc[7] += fin ? 0.0 : 1.0;
+        }
+    }
+    for (int k = 0; k < NDIAG; ++k) sh[threadIdx.x * NDIAG + k] = acc[k];
+    __syncthreads();
+    for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+        if ((int)threadIdx.x < s2) diag_combine(&sh[threadIdx.x * NDIAG], &sh[(threadIdx.x + s2) * NDIAG]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NDIAG; ++k) partials[blockIdx.x * NDIAG + k] = sh[k];
+}
+
 template <class R>
 cudaError_t launch_diag(const CPlanes<R>& u, int nx, int ny, int nz, double dx, double smallr, double* partials,
                         int nblocks, double* out, cudaStream_t s) {
+    bool quad = false;
+    if constexpr (std::is_same<R, float>::value) {
+        quad = nx % 4 == 0 && nx >= 8;
+        for (int v = 0; v < 9; ++v) quad = quad && (reinterpret_cast<uintptr_t>(u.p[v]) & 15u) == 0;
+    }
+    if constexpr (std::is_same<R, float>::value) {
+        if (quad) {
+            diag_kernel4<<<nblocks, 256, 0, s>>>(u, nx, ny, nz, dx, smallr, partials);
+            diag_final<<<1, 256, 0, s>>>(partials, nblocks, out);
+            return cudaGetLastError();
+        }
+    }
     diag_kernel<R><<<nblocks, 256, 0, s>>>(u, nx, ny, nz, dx, smallr, partials);
     diag_final<<<1, 256, 0, s>>>(partials, nblocks, out);
     return cudaGetLastError();

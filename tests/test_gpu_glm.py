@@ -218,3 +218,25 @@ def test_orszag_tang_gpu_fp32_pin():
     from glmmhdturb_b200 import turb
     d = turb.run_ot(N=64, t_end=0.2, dtype="f32")
     assert abs(d["vrms"] - 0.7887) < 5e-4 and abs(d["divbmax"] - 2.9) < 0.1, d
+
+
+def test_fp32_diagnostics_quad_pass_matches_fp64(oracle):
+    """The FP32 diagnostics read four cells per thread when nx is a multiple of 4 and the planes are
+    16-byte aligned, else one cell per thread; both accumulate in FP64, so on the same values they
+    match the FP64 diagnostics to summation-order round-off (max and min exactly)."""
+    from glmmhdturb_b200 import Solver
+    n = (64, 24, 20)
+    u0 = perturbed_glm_state(oracle, n, seed=11).astype(np.float32).astype(np.float64)
+    s64 = Solver(n, dtype="f64", gamma=5 / 3)
+    s32 = Solver(n, dtype="f32", gamma=5 / 3)
+    ref = s64.diagnostics(to_dev(u0))
+    u32 = to_dev(u0, torch.float32)
+    big = torch.empty(u32.numel() + 4, dtype=torch.float32, device="cuda")
+    mis = big[1:1 + u32.numel()].view(u32.shape)
+    mis.copy_(u32)
+    for got in (s32.diagnostics(u32), s32.diagnostics(mis)):
+        for k in ("mass", "ke2", "vrms", "divb_l2", "psi_l2", "etot"):
+            assert math.isclose(got[k], ref[k], rel_tol=1e-12), (k, got[k], ref[k])
+        for k in ("divbmax", "rhomin"):
+            assert got[k] == ref[k], (k, got[k], ref[k])
+        assert got["finite"] == 1 and got["nonfinite_cells"] == 0
