@@ -592,7 +592,10 @@ template <class R> __global__ void __launch_bounds__(256) ct_face_kernel4(const 
         const float4 ezq = ezc, eyq = eyc;
         const float ezn = __ldg(ez + cxn), eyn = __ldg(ey + cxn);
         const float4 ezx = make_float4(ezq.y, ezq.z, ezq.w, ezn), eyx = make_float4(eyq.y, eyq.z, eyq.w, eyn);
-        const float4 b5 = ld(A.q.p[5], c), b6 = ld(A.q.p[6], c), b7 = ld(A.q.p[7], c);
+        // the face field through the coherent path: its planes are the outputs' counterparts (the
+        // read-only cache is for data this kernel does not write)
+        auto ldc = [](const float* p, size_t i) { return *reinterpret_cast<const float4*>(p + i); };
+        const float4 b5 = ldc(A.q.p[5], c), b6 = ldc(A.q.p[6], c), b7 = ldc(A.q.p[7], c);
         float o5[4], o6[4], o7[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
