@@ -252,7 +252,7 @@ template <class R> struct MarchCell {
 template <class R, int RECON> struct MarchScheme {
     using Cell = MarchCell<R>;
     static constexpr bool kRecord = false;
-    static constexpr bool kEarlyOld = false;
+    static constexpr bool kEarlyOld = std::is_same<R, float>::value;   // 9.31 -> 9.15 ms at 512^3
     static __device__ __forceinline__ R prim_floor(const Consts<R>& K) { return K.smallp; }
     static __device__ __forceinline__ void recon(const R* PR, int PN, int, int c, int s0, int, int, const Consts<R>&, R,
                                                  Cell& r) {
