@@ -240,3 +240,20 @@ def test_fp32_diagnostics_quad_pass_matches_fp64(oracle):
         for k in ("divbmax", "rhomin"):
             assert got[k] == ref[k], (k, got[k], ref[k])
         assert got["finite"] == 1 and got["nonfinite_cells"] == 0
+
+
+def test_fp32_cfl_quad_pass_matches_one_cell_pass(oracle):
+    """The FP32 CFL reduction reads four cells per thread when every plane is 16-byte aligned, one
+    cell per thread otherwise; the per-cell signal speeds are the same, so the maxima are equal."""
+    from glmmhdturb_b200 import Solver
+    n = (64, 24, 20)
+    u0 = perturbed_glm_state(oracle, n, seed=12)
+    s32 = Solver(n, dtype="f32", gamma=5 / 3)
+    u32 = to_dev(u0, torch.float32)
+    big = torch.empty(u32.numel() + 4, dtype=torch.float32, device="cuda")
+    mis = big[1:1 + u32.numel()].view(u32.shape)
+    mis.copy_(u32)
+    a, b = s32.cfl(u32), s32.cfl(mis)
+    assert a == b and a[0] > 0.0
+    ref = oracle.cfl(oracle.Config(n=n, gamma=5 / 3), u0)
+    assert abs(a[0] - ref[0]) <= 1e-5 * ref[0] and abs(a[1] - ref[1]) <= 1e-5 * ref[1]
