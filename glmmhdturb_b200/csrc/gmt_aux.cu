@@ -109,12 +109,62 @@ __global__ void __launch_bounds__(256) ct_cfl_kernel(const CPlanes8<R> qv, int n
     block_max_atomic(sm, out + 1, red);
 }
 
+// FP32 CT CFL four cells x0..x0+3 (x0 = 4k) per thread: 16-byte loads, the +x face field of the
+// quad from the quad and the next cell of the row (periodic); maxima exactly the one-cell pass's
+__global__ void __launch_bounds__(256) ct_cfl_kernel4(const CPlanes8<float> qv, int nx, int ny, int nz,
+                                                      const Consts<float> K, unsigned long long* out) {
+    __shared__ double red[32];
+    const float* const* q = qv.p;
+    const size_t n = (size_t)nx * ny * nz, nq = n / 4;
+    auto ld = [](const float* p, size_t i) { return __ldg(reinterpret_cast<const float4*>(p + i)); };
+    auto el = [](const float4& v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); };
+    double cm = 0.0, sm = 0.0;
+    for (size_t qd = (size_t)blockIdx.x * blockDim.x + threadIdx.x; qd < nq; qd += (size_t)gridDim.x * blockDim.x) {
+        const size_t c = 4 * qd;
+        int x, y, z;
+        cell_coords(c, nx, ny, n, x, y, z);
+        const size_t iyp = (size_t)x + (size_t)nx * (wrap1(y + 1, ny) + (size_t)ny * z);
+        const size_t izp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrap1(z + 1, nz));
+        float4 v[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) v[k] = ld(q[k], c);
+        const float4 bx = ld(q[5], c), by = ld(q[6], c), bz = ld(q[7], c), byp = ld(q[6], iyp), bzp = ld(q[7], izp);
+        const float bxn = __ldg(q[5] + (x + 4 == nx ? c + 4 - nx : c + 4));
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            Q9<float> cc;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) cc.v[k] = el(v[k], j);
+            cc.v[5] = 0.5f * (el(bx, j) + (j < 3 ? el(bx, j + 1) : bxn));
+            cc.v[6] = 0.5f * (el(by, j) + el(byp, j));
+            cc.v[7] = 0.5f * (el(bz, j) + el(bzp, j));
+            cc.v[8] = 0.0f;
+            float ct, sg;
+            cfl_speeds(cc, K, ct, sg);
+            cm = fmax(cm, (double)ct);
+            sm = fmax(sm, (double)sg);
+        }
+    }
+    block_max_atomic(cm, out, red);
+    __syncthreads();
+    block_max_atomic(sm, out + 1, red);
+}
+
 template <class R>
 cudaError_t launch_ct_cfl(const CPlanes8<R>& q, int nx, int ny, int nz, const Consts<R>& K, unsigned long long* out,
                           cudaStream_t s) {
     size_t n = (size_t)nx * ny * nz;
-    int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
     cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), s);
+    if constexpr (std::is_same<R, float>::value) {
+        bool quad = nx % 4 == 0;
+        for (int v = 0; v < 8; ++v) quad = quad && (reinterpret_cast<uintptr_t>(q.p[v]) & 15u) == 0;
+        if (quad) {
+            const int nb4 = (int)std::min<size_t>((n / 4 + 255) / 256, 148 * 8);
+            ct_cfl_kernel4<<<nb4, 256, 0, s>>>(q, nx, ny, nz, K, out);
+            return cudaGetLastError();
+        }
+    }
+    int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
     ct_cfl_kernel<R><<<nb, 256, 0, s>>>(q, nx, ny, nz, K, out);
     return cudaGetLastError();
 }

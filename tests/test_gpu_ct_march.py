@@ -344,3 +344,16 @@ def test_fp32_quad_passes_match_one_cell_passes():
     assert torch.equal(w[:9], wm[:9])
     d = (w[9:] - wm[9:]).abs().max().item()
     assert d <= 1e-6 * w[9:].abs().max().item(), d
+
+
+def test_fp32_ct_cfl_quad_pass_matches_one_cell_pass():
+    """The FP32 CT CFL reduction (cell-centred field from the face field) reads four cells per
+    thread on aligned planes and one cell per thread otherwise; the maxima are equal."""
+    from glmmhdturb_b200 import Solver
+    n = (64, 32, 16)
+    s = Solver(n, dtype="f32", scheme="ct", recon="mc", riemann="hlld", emf="contact", gamma=5 / 3)
+    q = s.alloc()
+    s.ic_turbulent(q, mach=1.5, seed=5)
+    a = s.cfl(q)
+    b = s.cfl(_offset_copy(q))
+    assert a == b and a[0] > 0.0
