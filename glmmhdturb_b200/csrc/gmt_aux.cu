@@ -88,7 +88,8 @@ __global__ void __launch_bounds__(256) ct_cfl_kernel(const CPlanes8<R> qv, int n
     size_t n = (size_t)nx * ny * nz;
     double cm = 0.0, sm = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        int x, y, z;
+        cell_coords(i, nx, ny, n, x, y, z);   // 32-bit divisions below 2^32 cells
         size_t ixp = (size_t)wrapi(x + 1, nx) + (size_t)nx * (y + (size_t)ny * z);
         size_t iyp = (size_t)x + (size_t)nx * (wrapi(y + 1, ny) + (size_t)ny * z);
         size_t izp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrapi(z + 1, nz));
@@ -188,7 +189,8 @@ __global__ void __launch_bounds__(256) diag_kernel(const CPlanes<R> u, int nx, i
     double acc[NDIAG] = {0, 0, 0, 0, 0, 0, 1e300, 0};
     const size_t n = (size_t)nx * ny * nz;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        int x, y, z;
+        cell_coords(i, nx, ny, n, x, y, z);   // 32-bit divisions below 2^32 cells
         double rho = (double)u.p[0][i], mx = (double)u.p[1][i], my = (double)u.p[2][i], mz = (double)u.p[3][i];
         double ps = (double)u.p[8][i];
         acc[0] += rho;
@@ -319,7 +321,8 @@ __global__ void __launch_bounds__(256) ct_divb_kernel(const CPlanes8<R> qv, int 
     size_t n = (size_t)nx * ny * nz;
     double m = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        int x, y, z;
+        cell_coords(i, nx, ny, n, x, y, z);   // 32-bit divisions below 2^32 cells
         size_t ixp = (size_t)wrapi(x + 1, nx) + (size_t)nx * (y + (size_t)ny * z);
         size_t iyp = (size_t)x + (size_t)nx * (wrapi(y + 1, ny) + (size_t)ny * z);
         size_t izp = (size_t)x + (size_t)nx * (y + (size_t)ny * wrapi(z + 1, nz));
